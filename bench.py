@@ -1,0 +1,369 @@
+#!/usr/bin/env python3
+"""Benchmark of the law-step hot path on B200: the 7-point FP32 heat step, d T = diffuse(1, T), conserves T, at 512^3.
+
+One step = one explicit Euler step of the whole 512^3 lattice (one substep: dt = 0.4 h^2 / 6 is exactly max_dt), with
+the conserved-total, range/NaN, bounds and change contracts checked on the card in the same pass. Metric: effective
+HBM bandwidth at the reference's own unit of 8 bytes a cell a step (one fp32 read and one write), against the measured
+copy roof.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--size 512]
+
+Prints ONE JSON line (rank 0). With --gpus N > 1 (torchrun), every rank steps its own 512^3 lattice (independent
+instances, no data-path collective: weak scaling), timed with CUDA events, max over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "online-physics-cuda_b200")
+sys.path.insert(0, PKG)
+sys.path.insert(0, ROOT)
+
+BYTES_PER_CELL = 8  # one fp32 read of T and one write of the next T (the reference's unit, stencil_bench.cpp:188)
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(name):
+    """dram bytes per launch of the dominant kernel from the committed ncu summary (profiles/<name>.md), or None."""
+    path = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        if shutil.which("nvidia-smi") is None:
+            return
+        self.out = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                      "-i", str(self.index), "-lms", "100"], stdout=self.out, stderr=subprocess.DEVNULL)
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        self.out.seek(0)
+        rows = [r.split(",") for r in self.out.read().strip().splitlines() if r.strip()]
+        os.unlink(self.out.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def init_dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---- the reference's CPU solver (the oracle built from the reference's sources), timed on this host ----------------
+
+HEAT_LAW = """field T init 0 range -1000000 1000000
+param D = 1
+term conduction
+  d T = diffuse(D, T)
+  conserves T
+  max_dt = 0.4 * h * h / (6 * D)
+"""
+
+
+def cpu_reference_heat(n, steps, warmup, threads):
+    """Times the reference's own OpenMP CPU solver (oracle/_ref/lawc) on the heat law at n^3. Returns (ms/step, kind,
+    cores) or None when the binary is absent. Falls back to nothing: the oracle port is in oracle/heat.py."""
+    lawc = os.path.join(ROOT, "oracle", "_ref", "lawc")
+    if not os.path.exists(lawc):
+        return None
+    import numpy as np
+    from oracle import heat as oh
+    h = 1.0 / n
+    dt = 0.4 * h * h / 6.0
+    work = tempfile.mkdtemp(prefix="fe_cpu_")
+    try:
+        law = os.path.join(work, "heat.law")
+        open(law, "w").write(HEAT_LAW)
+        scene = os.path.join(work, "heat.scene")
+        open(scene, "w").write(f"grid {n} {n} {n} {h!r}\nlaw {law}\n")
+        init = os.path.join(work, "init")
+        os.makedirs(init)
+        oh.gaussian_blobs(n, h, seed=0).tofile(os.path.join(init, "T.bin"))
+        out = os.path.join(work, "t.json")
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        subprocess.run([lawc, "--scene", scene, "--init", init, "--steps", str(steps + warmup), "--dt", repr(dt),
+                        "--json", out, "--warmup", str(warmup)], check=True, env=env, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.DEVNULL)
+        ms = json.load(open(out))["mean_ms"]
+        return ms, "reference", threads
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    n = args.size
+    threads = os.cpu_count() or 1
+    steps = args.steps
+    # Bounded: each CPU step at 512^3 takes seconds; cap the sample so the run ends within a few minutes.
+    cells = n ** 3
+    sample_steps = max(1, min(steps, int(60e9 / (cells * 40))))
+    res = cpu_reference_heat(n, sample_steps, min(args.warmup, 1), threads)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/lawc (the reference's CPU solver) is not built"}))
+        return
+    ms, kind, cores = res
+    gbs = BYTES_PER_CELL * cells / (ms * 1e-3) / 1e9
+    sample = f"{sample_steps} timed steps of the {n}^3 heat law after 1 warm-up, reference lawc, OMP_NUM_THREADS={cores}"
+    print(json.dumps({
+        "impl": "reference", "metric": "7-pt stencil effective HBM GB/s (8 B/cell/step)", "value": gbs, "unit": "GB/s",
+        "n_gpus": world, "steps": sample_steps, "warmup": 1, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"heat 7-pt diffuse(D=1,T) {n}^3 fp32, conserves T, 1 substep, contracts on",
+                   "cells": cells},
+        "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ---- our arm ---------------------------------------------------------------------------------------------------------
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    from fieldcuda import _lib, kernels
+    from oracle import heat as oh
+
+    torch.cuda.set_device(local)
+    _lib.check(_lib.lib().fe_device_check())
+    n = args.size
+    h = 1.0 / n
+    dt = 0.4 * h * h / 6.0
+    cells = n ** 3
+    variant, zchunk = args.variant, args.zchunk
+    stream = torch.cuda.Stream()
+    T0 = oh.gaussian_blobs(n, h, seed=rank)
+    host = torch.from_numpy(T0).pin_memory()
+    a = torch.empty((n, n, n), dtype=torch.float32, device="cuda")
+    b = torch.empty_like(a)
+    K, W = args.steps, args.warmup
+    # One workspace (contract record + per-block partials) per timed step: records are judged after the run, so no
+    # step waits on the host.
+    ws = [kernels.heat7_workspace((n, n, n), variant, zchunk) for _ in range(max(K, W))]
+    check = _lib.FE_HEAT7_BEFORE | _lib.FE_HEAT7_AFTER
+    flags = dict(lo=-1e6, hi=1e6, variant=variant, zchunk=zchunk, check=check)
+
+    with torch.cuda.stream(stream):
+        a.copy_(host, non_blocking=True)
+        for i in range(W):
+            kernels.check_reset(ws[i], stream)
+            kernels.heat7_step(a, b, 1.0, h, dt, workspace=ws[i], stream=stream, **flags)
+            a, b = b, a
+        stream.synchronize()
+
+        # Copy roof in the same run: a device-to-device copy of the same bytes.
+        ca = torch.empty(cells, dtype=torch.float32, device="cuda")
+        cb = torch.empty_like(ca)
+        for _ in range(3):
+            kernels.copy_f32(ca, cb, stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(10):
+            kernels.copy_f32(ca, cb, stream)
+        e1.record(stream)
+        stream.synchronize()
+        copy_gbs = 2 * 4 * cells * 10 / (e0.elapsed_time(e1) * 1e-3) / 1e9
+        del ca, cb
+
+        clocks = ClockSampler(torch.cuda.current_device())
+        clocks.start()
+        barrier(world)
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for i in range(K):
+            kernels.check_reset(ws[i], stream)
+            kernels.heat7_step(a, b, 1.0, h, dt, workspace=ws[i], stream=stream, **flags)
+            a, b = b, a
+        end.record(stream)
+        stream.synchronize()
+        torch.cuda.synchronize()
+        barrier(world)
+        clk = clocks.stop()
+        ms_total = start.elapsed_time(end)
+        ms_total = max_over_ranks(world, ms_total)
+        recs = [kernels.check_read(ws[i], stream) for i in range(K)]
+        # Judge the conserved-total contract of every timed step (Solver.cpp:439-453's tolerance).
+        worst = 0.0
+        for r in recs:
+            tol = 1e-5 * (r.before_abs + 1.0)
+            worst = max(worst, abs(r.after - r.before) / tol)
+            assert r.out_of_range == 0 and r.not_finite == 0
+        assert worst <= 1.0, f"conservation broken: {worst}"
+
+        # End to end through the C ABI with host buffers: the initial state up from pinned host memory, K steps, each
+        # step's contract record read back to the host, the final state back down.
+        rec_host = torch.empty((K, 128), dtype=torch.uint8).pin_memory()
+        out_host = torch.empty((n, n, n), dtype=torch.float32).pin_memory()
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        a.copy_(host, non_blocking=True)
+        for i in range(K):
+            kernels.check_reset(ws[i], stream)
+            kernels.heat7_step(a, b, 1.0, h, dt, workspace=ws[i], stream=stream, **flags)
+            rec_host[i].copy_(ws[i][:128], non_blocking=True)
+            a, b = b, a
+        out_host.copy_(a, non_blocking=True)
+        e3.record(stream)
+        stream.synchronize()
+        e2e_ms = max_over_ranks(world, e2.elapsed_time(e3))
+        wall_e2e_ms = (time.perf_counter() - t0) * 1e3
+
+    ms_step = ms_total / K
+    total_cells = cells * world
+    value = BYTES_PER_CELL * total_cells * K / (ms_total * 1e-3) / 1e9
+    e2e_value = BYTES_PER_CELL * total_cells * K / (e2e_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak()
+    per_launch_achieved = BYTES_PER_CELL * cells / (ms_step * 1e-3) / 1e9
+    traffic = profile_traffic("heat7_tma_512.md")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        res = cpu_reference_heat(n, 2, 1, threads)
+        if res is not None:
+            ms, kind, cores = res
+            cpu = {"value": BYTES_PER_CELL * cells / (ms * 1e-3) / 1e9, "unit": "GB/s", "cores": cores, "kind": kind,
+                   "sample": f"2 timed steps of the {n}^3 heat law after 1 warm-up (reference lawc, its OpenMP solver)"}
+        else:
+            t = time.perf_counter()
+            oh.cpu_step(T0, 1.0, h, dt)
+            ms = (time.perf_counter() - t) * 1e3
+            cpu = {"value": BYTES_PER_CELL * cells / (ms * 1e-3) / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
+                   "sample": f"1 step of the {n}^3 heat law, numpy restatement (oracle/heat.py)"}
+
+    if rank != 0:
+        return
+    print(json.dumps({
+        "metric": "7-pt stencil effective HBM GB/s (8 B/cell/step)",
+        "value": value, "unit": "GB/s", "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: sum of 4 seeded Gaussian blobs (numpy default_rng(rank))",
+        "config": {"workload": f"heat 7-pt diffuse(D=1,T) {n}^3 fp32, conserves T, 1 substep, contracts fused and "
+                               f"judged for every step", "cells_per_gpu": cells, "kernel": f"heat7_tma variant {variant}",
+                   "zchunk": zchunk, "l2": "inputs larger than L2 (512 MiB a buffer)"},
+        "roofline": {"bound": "hbm", "achieved": per_launch_achieved, "peak": peak, "unit": "GB/s",
+                     "frac": per_launch_achieved / peak, "traffic": traffic,
+                     "peak_source": f"{peak_kind} copy (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                     "copy_same_run_gbs": copy_gbs},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": 4 * cells // K,
+                "d2h_bytes_per_step": 128 + 4 * cells // K, "wall_ms": wall_e2e_ms,
+                "what": "initial state H2D from pinned host, K steps, each step's contract record D2H, final state D2H"},
+        "gpu_launches": K,
+        "clocks": clk,
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=512)
+    ap.add_argument("--variant", type=int, default=0)
+    ap.add_argument("--zchunk", type=int, default=64)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = init_dist()
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,33 @@
+// Host-side interface of the hand-written kernels in heat7.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "fe_device.cuh"
+
+namespace fe {
+
+struct HeatArgs {
+    float* out;
+    int nx, ny, nz;
+    int zchunk;
+    float k, h, dt;
+    float lo, hi;       // the field's declared range (range contract)
+    int totals_before;  // this pass starts the term: record the totals before it
+    int totals_after;   // this pass ends the term: record the totals after it
+    FeCheck* rec;       // null: no contracts in this pass
+    double* partials;   // 4 doubles a block
+    unsigned* count;    // blocks finished (reset by the last)
+    unsigned* err;      // error word (bounded waits)
+};
+
+cudaError_t launch_heat7_tma(int variant, const FeTensorMap& map, const HeatArgs& a, cudaStream_t stream);
+cudaError_t launch_heat7_plain(const float* T, const HeatArgs& a, cudaStream_t stream);
+cudaError_t launch_copy(const float* a, float* b, size_t n, int sms, cudaStream_t stream);
+int heat7_tma_rows(int variant);
+int heat7_tma_blocks(int variant, int nx, int ny, int nz, int zchunk);
+int heat7_plain_blocks(int nx, int ny, int nz, int zchunk);
+
+} // namespace fe
