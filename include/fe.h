@@ -78,6 +78,104 @@ int fe_check_read(const void* workspace, fe_check* out, void* stream);
 /* A device-to-device copy of n floats (n a multiple of 4, 16-byte aligned): the bandwidth roof for the roofline. */
 int fe_copy_f32(const float* src_dev, float* dst_dev, size_t n, void* stream);
 
+/* ---- the law backend ------------------------------------------------------------------------------------------------
+ * A law (the reference's .law text, unchanged) compiled for one lattice nx*ny*nz of cell size h: parsed, lowered to the
+ * SSA IR with the reference's rules, turned into sm_100a kernels (NVRTC), with its fields on the card. The handle is
+ * single-threaded; handles are independent (each has its own stream). Replaces the reference's CudaSolver behind its
+ * LawBackend interface (src/field/Backend.hpp:67-84; src/field/cuda/CudaSolver.cpp:46-1167). */
+typedef struct fe_law fe_law;
+
+/* Violation kinds (Violation::Kind, src/field/Backend.hpp:16-22). */
+#define FE_RANGE 0
+#define FE_NOT_FINITE 1
+#define FE_CONSERVATION 2
+#define FE_SUBSTEP_CAP 3
+
+typedef struct fe_violation {
+    int kind;
+    int term;            /* the term's index, -1 for a derive */
+    int field;           /* the field (the first of a conserved group), -1 for a substep cap */
+    uint32_t count;      /* cells out of range / not finite */
+    uint32_t first_cell; /* linear index (x fastest) of the first bad cell */
+    double before, after, tolerance; /* conservation: the group's totals and the tolerance */
+    long long step;      /* the step (0-based) the records belong to */
+    char detail[160];
+} fe_violation;
+
+typedef struct fe_step_info {
+    int violations;      /* violations now held (fe_law_violation) */
+    int launches;        /* kernels the step launched */
+    double gpu_ms;       /* the step's device time (0 when it did not wait for the card) */
+} fe_step_info;
+
+typedef struct fe_field_info {
+    double init, lo, hi;
+    int is_static, derived, clamp;
+} fe_field_info;
+
+/* Step flags. */
+#define FE_STEP_IGNORE_MAX_DT 1 /* Solver::set_respect_max_dt(false): the falsification hook (Solver.hpp:91-93) */
+
+/* Compiles `law_text` (one or more law sources joined; `source_name` names it in errors) for the lattice and puts its
+ * fields on the current device at their `init` values. FE_ELAW with the compiler's messages, FE_EUNSUP for ops this
+ * backend does not run. Replaces CudaSolver::create (src/field/cuda/CudaSolver.hpp:27, CudaSolver.cpp:1143-1152). */
+int fe_law_create(const char* law_text, const char* source_name, int nx, int ny, int nz, double h, fe_law** out);
+void fe_law_destroy(fe_law* law);
+
+/* Compile-only services, no device needed: the IR as the reference's JSON (lawc --ir-json, src/field/ir/LawIR.cpp:528-593)
+ * or listing (lawc --ir, LawIR.cpp:595-656), and the generated CUDA translation unit (lawc --cuda, CudaSolver::source).
+ * Text goes to buf (capacity cap, NUL-terminated); *needed gets the full length + 1. fe_law_compile_check also runs NVRTC
+ * on the generated source (no GPU needed). */
+int fe_law_ir_json(const char* law_text, char* buf, size_t cap, size_t* needed);
+int fe_law_ir_listing(const char* law_text, char* buf, size_t cap, size_t* needed);
+int fe_law_source(const char* law_text, int nx, int ny, int nz, double h, char* buf, size_t cap, size_t* needed);
+int fe_law_compile_check(const char* law_text, int nx, int ny, int nz, double h);
+
+/* Fields and params (Law::field_id / param_id, Solver::set_param; src/field/Law.hpp:196-199, Solver.hpp:55-56). */
+int fe_law_field_count(const fe_law* law);
+int fe_law_field_id(const fe_law* law, const char* name);
+int fe_law_field_name(const fe_law* law, int field, char* buf, size_t cap);
+int fe_law_field_info(const fe_law* law, int field, fe_field_info* out);
+int fe_law_term_count(const fe_law* law);
+int fe_law_term_name(const fe_law* law, int term, char* buf, size_t cap);
+int fe_law_param_count(const fe_law* law);
+int fe_law_param_id(const fe_law* law, const char* name);
+int fe_law_set_param(fe_law* law, int param, double value);
+int fe_law_get_param(const fe_law* law, int param, double* value);
+
+/* Whole-field transfers (the host FieldSet <-> the card; FieldEdits::all and LawBackend::fetch, Backend.hpp:31-40, 79).
+ * `host` holds nx*ny*nz floats, x fastest. The _device forms copy from / to a device buffer of the same size. */
+int fe_law_upload(fe_law* law, int field, const float* host);
+int fe_law_upload_device(fe_law* law, int field, const float* dev);
+int fe_law_fetch(fe_law* law, int field, float* host);
+int fe_law_fetch_device(fe_law* law, int field, float* dev);
+/* The card's current buffer of a field (valid until the next step). */
+int fe_law_field_device_ptr(const fe_law* law, int field, const float** dev);
+
+/* One step of dt: every term in declaration order with its substeps, then the derives (Solver::step,
+ * src/field/Solver.cpp:273-285; LawBackend::step). With contracts checked this step (fe_law_check_every) and not
+ * deferred, waits for the card and judges them: fe_law_violation reads what broke. */
+int fe_law_step(fe_law* law, double dt, int flags, fe_step_info* info);
+/* Recomputes the derived fields (LawBackend::derive, Solver::refresh_derived). */
+int fe_law_derive(fe_law* law);
+/* Contracts looked at one step in `steps` (LawBackend::check_contracts_every). */
+int fe_law_check_every(fe_law* law, int steps);
+/* Deferred judging: checked steps keep their records on the card (up to 63 steps) and fe_law_sync judges them; the
+ * steps then never wait for the host. Violations carry the step they belong to. */
+int fe_law_set_deferred(fe_law* law, int on);
+int fe_law_sync(fe_law* law, fe_step_info* info);
+int fe_law_violation(const fe_law* law, int index, fe_violation* out);
+/* Substeps term `term` took in the last step (Solver::last_substeps). */
+int fe_law_substeps(const fe_law* law, int term);
+/* Whether the term did nothing in the last step (its bounds said idle; TermProfile::idle). */
+int fe_law_term_idle(const fe_law* law, int term);
+/* FNV-1a over every field's bits in declaration order (FieldSet::digest, src/field/Grid.cpp:60-77). */
+int fe_law_digest(fe_law* law, uint64_t* out);
+/* The handle's stream (a cudaStream_t), for callers that order their own work after its steps. */
+int fe_law_stream(const fe_law* law, void** stream);
+/* Device time of `launches` back-to-back launches of term `term`'s fused gather pass (the roofline's kernel). */
+int fe_law_time_gather(fe_law* law, int term, int launches, float* ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,6 +6,7 @@
 #include "cuda_ctx.hpp"
 #include "heat7.hpp"
 
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -54,6 +55,16 @@ MapCache& map_cache()
 }
 
 constexpr std::size_t kCheckHeader = 128; // fe_check (64 bytes), error word, block counter, padding
+
+// 1/v when v is a power of two whose reciprocal is a normal float (then x / v == x * (1/v) to the bit), else 0.
+float exact_reciprocal(float v)
+{
+    int e = 0;
+    const float m = std::frexp(v, &e);
+    if (!(v > 0.0f) || m != 0.5f) return 0.0f;
+    const float r = 1.0f / v;
+    return std::isnormal(r) ? r : 0.0f;
+}
 
 } // namespace
 
@@ -188,6 +199,7 @@ int fe_heat7_step(const float* T_dev, float* out_dev, int nx, int ny, int nz, fl
     a.k = k;
     a.h = h;
     a.dt = dt;
+    a.inv_hh = exact_reciprocal(h * h);
     a.lo = lo;
     a.hi = hi;
     a.totals_before = (check & FE_HEAT7_BEFORE) ? 1 : 0;

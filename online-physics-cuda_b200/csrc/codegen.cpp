@@ -1,0 +1,758 @@
+#include "codegen.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <functional>
+#include <map>
+#include <set>
+#include <sstream>
+
+namespace fe::gen {
+
+const char* device_prelude()
+{
+    static const char* text =
+#include "fe_device_prelude.inc"
+        ;
+    return text;
+}
+
+namespace {
+
+using ir::Inst;
+using ir::Shape;
+using law::Op;
+
+// A float literal as the reference prints it (%.9g of the float value; CudaCodegen.cpp:278-295).
+std::string literal(double v)
+{
+    if (!std::isfinite(v)) return v > 0 ? "1e30f" : (v < 0 ? "(-1e30f)" : "0.f");
+    const float f = static_cast<float>(v);
+    if (!std::isfinite(f)) return f > 0 ? "__int_as_float(0x7f800000)" : "__int_as_float(0xff800000)";
+    char text[48];
+    std::snprintf(text, sizeof(text), "%.9g", static_cast<double>(f));
+    std::string s = text;
+    if (s.find_first_of(".eEn") == std::string::npos) s += ".0";
+    return "(" + s + "f)";
+}
+
+struct Radius {
+    int x = 0, y = 0, z = 0;
+};
+
+// How far along each axis an op reads its arguments from its own cell.
+Radius axis_radius(const Inst& in)
+{
+    switch (in.op) {
+    case Op::Shift: case Op::ShiftT:
+        return {std::abs(in.offset[0]), std::abs(in.offset[1]), std::abs(in.offset[2])};
+    case Op::Lap: case Op::Diffuse: case Op::Adv: case Op::Topple:
+        return {1, 1, 1};
+    case Op::Gx: case Op::GxT: return {1, 0, 0};
+    case Op::Gy: case Op::GyT: return {0, 1, 0};
+    case Op::Gz: case Op::GzT: return {0, 0, 1};
+    case Op::Fall: return {0, 0, 1};
+    case Op::Spread: return {1, 1, 0};
+    default: return {};
+    }
+}
+
+bool supported_cell_op(Op op)
+{
+    switch (op) {
+    case Op::Distance: case Op::Poisson: case Op::Mlp: case Op::Flux: case Op::LDiffuse: case Op::Local:
+        return false;
+    default:
+        return true;
+    }
+}
+
+class Generator {
+public:
+    Generator(const ir::Module& m, const law::Law& law, int nx, int ny, int nz, double h, Plan& plan)
+        : m_(m), law_(law), nx_(nx), ny_(ny), nz_(nz), h_(h), plan_(plan)
+    {
+    }
+
+    bool run(std::string& why)
+    {
+        plan_.slot_of.assign(m_.insts.size(), -1);
+        plan_.uniform_of.assign(m_.insts.size(), -1);
+        plan_.pingpong.assign(law_.fields.size(), 0);
+        if (!allocate(why)) return false;
+        out_ << device_prelude() << "\n";
+        out_ << "__constant__ float FE_P[1024];\n";
+        out_ << "__device__ float FE_U[" << std::max(plan_.uniforms, 1) << "];\n";
+        out_ << "constexpr int NX = " << nx_ << ", NY = " << ny_ << ", NZ = " << nz_ << ";\n";
+        out_ << "constexpr float FE_H = " << literal(h_) << ";\n";
+        out_ << R"(__device__ __forceinline__ int fe_ex(int v) { return v < 0 ? 0 : (v >= NX ? NX - 1 : v); }
+__device__ __forceinline__ int fe_ey(int v) { return v < 0 ? 0 : (v >= NY ? NY - 1 : v); }
+__device__ __forceinline__ int fe_ez(int v) { return v < 0 ? 0 : (v >= NZ ? NZ - 1 : v); }
+__device__ __forceinline__ bool fe_inside(int x, int y, int z) { return x >= 0 && y >= 0 && z >= 0 && x < NX && y < NY && z < NZ; }
+__device__ __forceinline__ int fe_imin(int a, int b) { return a < b ? a : b; }
+__device__ __forceinline__ int fe_imax(int a, int b) { return a > b ? a : b; }
+__device__ __forceinline__ void fe_run_to(int j, int d, int n, int& lo, int& hi)
+{
+    lo = fe_imax(j == 0 ? 0 : j - d, 0); hi = fe_imin(j == n - 1 ? n - 1 : j - d, n - 1);
+}
+__device__ __forceinline__ float fe_dv(float a, float b) { return b == 0.f ? 0.f : a / b; }
+__device__ __forceinline__ float fe_sat(float v) { return fminf(fmaxf(v, 0.f), 1.f); }
+__device__ __forceinline__ float fe_face(float ka, float kb, float va, float vb)
+{
+    const float s = ka + kb;
+    return (s > 0.f ? 2.f * ka * kb / s : 0.f) * (vb - va);
+}
+)";
+        for (std::size_t t = 0; t < m_.terms.size(); ++t) {
+            if (!program(m_.terms[t], "t" + std::to_string(t), false, plan_.terms.emplace_back(), why)) return false;
+            if (!program(m_.learned[t], "l" + std::to_string(t), false, plan_.learned.emplace_back(), why)) return false;
+        }
+        for (std::size_t d = 0; d < m_.derives.size(); ++d) {
+            if (!program(m_.derives[d], "d" + std::to_string(d), true, plan_.derives.emplace_back(), why)) return false;
+        }
+        plan_.source = out_.str();
+        return true;
+    }
+
+private:
+    [[nodiscard]] const Inst& at(int id) const { return m_.insts[static_cast<std::size_t>(id)]; }
+
+    bool allocate(std::string& why)
+    {
+        std::set<int> used;
+        auto take = [&](const ir::Program& p) {
+            used.insert(p.stages.begin(), p.stages.end());
+            used.insert(p.limit_stages.begin(), p.limit_stages.end());
+        };
+        for (const ir::Program& p : m_.terms) take(p);
+        for (const ir::Program& p : m_.learned) take(p);
+        for (const ir::Program& p : m_.derives) take(p);
+        for (const int id : used) {
+            const Inst& in = at(id);
+            switch (in.op) {
+            case Op::Tridiag:
+                plan_.slot_of[static_cast<std::size_t>(id)] = plan_.slots;
+                plan_.slots += 2; // the answer, and c' of the y/z recurrence
+                break;
+            case Op::MaxOf: case Op::MinOf: case Op::SumOf:
+                plan_.uniform_of[static_cast<std::size_t>(id)] = plan_.uniforms++;
+                break;
+            case Op::Distance: case Op::Poisson: case Op::Mlp: case Op::Flux: case Op::LDiffuse:
+                why = std::string("this backend does not run '") + law::op_name(in.op) + "' stages yet";
+                return false;
+            default:
+                plan_.slot_of[static_cast<std::size_t>(id)] = plan_.slots++;
+                break;
+            }
+        }
+        for (const Inst& in : m_.insts) {
+            if (!supported_cell_op(in.op)) {
+                why = std::string("this backend does not run '") + law::op_name(in.op) + "' yet";
+                return false;
+            }
+        }
+        if (m_.insts.empty()) return true;
+        return true;
+    }
+
+    // ---- one pass: its sources, their halos, and its device code ------------------------------------------------------
+
+    struct PassBuild {
+        std::vector<Source> sources;
+        std::vector<Radius> reach;            // per source
+        std::set<int> own_stages;             // stages whose bodies this pass computes
+        std::set<std::pair<int, std::tuple<int, int, int>>> seen;
+    };
+
+    int source_index(PassBuild& pb, Buf buf)
+    {
+        for (std::size_t k = 0; k < pb.sources.size(); ++k) {
+            if (pb.sources[k].buf == buf) return static_cast<int>(k);
+        }
+        pb.sources.push_back(Source{buf});
+        pb.reach.push_back({});
+        return static_cast<int>(pb.sources.size()) - 1;
+    }
+
+    // Walks a value's inlined closure with the offset it is read at, growing the sources' reach. `body`: evaluate this
+    // instruction itself even if it is a stage (the stage a pass stores); otherwise a stage is a read of its slot.
+    void walk(PassBuild& pb, int id, Radius off, bool body)
+    {
+        const Inst& in = at(id);
+        if (!pb.seen.insert({id * 2 + (body ? 1 : 0), {off.x, off.y, off.z}}).second) return;
+        const bool stored = m_.is_stage(id) || in.global;
+        if (!body && stored) {
+            if (in.shape == Shape::Scalar) return; // a reduction's uniform
+            const int k = source_index(pb, Buf{Buf::Slot, plan_.slot_of[static_cast<std::size_t>(id)]});
+            Radius& r = pb.reach[static_cast<std::size_t>(k)];
+            r.x = std::max(r.x, off.x);
+            r.y = std::max(r.y, off.y);
+            r.z = std::max(r.z, off.z);
+            return;
+        }
+        if (in.op == Op::Field) {
+            const int k = source_index(pb, Buf{Buf::FieldNow, in.index});
+            Radius& r = pb.reach[static_cast<std::size_t>(k)];
+            r.x = std::max(r.x, off.x);
+            r.y = std::max(r.y, off.y);
+            r.z = std::max(r.z, off.z);
+            return;
+        }
+        const Radius a = axis_radius(in);
+        const Radius next{off.x + a.x, off.y + a.y, off.z + a.z};
+        for (const int arg : in.args) walk(pb, arg, next, false);
+    }
+
+    // The device functions of a pass: v<id>(c, x, y, z) for every instruction its outputs inline (stages it reads, and
+    // fields, are loads of their source) and b<id> for the bodies of the stages it stores.
+    void emit_functions(std::ostringstream& f, PassBuild& pb, const std::vector<int>& roots, bool bodies)
+    {
+        std::set<int> done;
+        std::vector<std::pair<int, bool>> order;
+        std::function<void(int, bool)> visit = [&](int id, bool body) {
+            const int key = id * 2 + (body ? 1 : 0);
+            if (done.count(key)) return;
+            const Inst& in = at(id);
+            const bool stored = (m_.is_stage(id) || in.global) && !body;
+            if (!stored) {
+                for (const int a : in.args) visit(a, false);
+            }
+            done.insert(key);
+            order.emplace_back(id, body);
+        };
+        for (const int r : roots) visit(r, bodies);
+        for (const auto& [id, body] : order) emit_inst(f, pb, id, body);
+    }
+
+    static std::string v(int id, const std::string& x = "x", const std::string& y = "y", const std::string& z = "z")
+    {
+        return "v" + std::to_string(id) + "(c, " + x + ", " + y + ", " + z + ")";
+    }
+
+    void emit_inst(std::ostringstream& f, PassBuild& pb, int id, bool body)
+    {
+        const Inst& in = at(id);
+        const std::string name = (body ? "b" : "v") + std::to_string(id);
+        f << "template <class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)";
+        auto a = [&](std::size_t k, const std::string& x = "x", const std::string& y = "y", const std::string& z = "z") {
+            return v(in.args[k], x, y, z);
+        };
+        auto simple = [&](const std::string& e) { f << " { return " << e << "; }\n"; };
+        const bool stored = (m_.is_stage(id) || in.global) && !body;
+        if (stored) {
+            if (in.shape == Shape::Scalar) {
+                simple("FE_U[" + std::to_string(plan_.uniform_of[static_cast<std::size_t>(id)]) + "]");
+            } else {
+                const int k = source_index(pb, Buf{Buf::Slot, plan_.slot_of[static_cast<std::size_t>(id)]});
+                simple("c.template ld<" + std::to_string(k) + ">(x, y, z)");
+            }
+            return;
+        }
+        switch (in.op) {
+        case Op::Const: simple(literal(in.number)); break;
+        case Op::Param: simple("FE_P[" + std::to_string(in.index) + "]"); break;
+        case Op::Cell: simple("FE_H"); break;
+        case Op::Dt: simple("c.dt"); break;
+        case Op::Rim: simple("(x == 0 || y == 0 || z == 0 || x + 1 == NX || y + 1 == NY || z + 1 == NZ) ? 1.f : 0.f"); break;
+        case Op::Local: simple("0.f"); break;
+        case Op::Field: {
+            const int k = source_index(pb, Buf{Buf::FieldNow, in.index});
+            simple("c.template ld<" + std::to_string(k) + ">(x, y, z)");
+            break;
+        }
+        case Op::Neg: simple("-" + a(0)); break;
+        case Op::Abs: simple("fabsf(" + a(0) + ")"); break;
+        case Op::Sqrt: simple("sqrtf(fmaxf(0.f, " + a(0) + "))"); break;
+        case Op::Exp: simple("expf(fminf(" + a(0) + ", 80.f))"); break;
+        case Op::Log: simple("logf(fmaxf(" + a(0) + ", 1e-30f))"); break;
+        case Op::Step: simple(a(0) + " > 0.f ? 1.f : 0.f"); break;
+        case Op::Pos: simple("fmaxf(" + a(0) + ", 0.f)"); break;
+        case Op::Add: simple(a(0) + " + " + a(1)); break;
+        case Op::Sub: simple(a(0) + " - " + a(1)); break;
+        case Op::Mul: simple(a(0) + " * " + a(1)); break;
+        case Op::Div: simple("fe_dv(" + a(0) + ", " + a(1) + ")"); break;
+        case Op::Pow: simple("powf(" + a(0) + ", " + a(1) + ")"); break;
+        case Op::Min: simple("fminf(" + a(0) + ", " + a(1) + ")"); break;
+        case Op::Max: simple("fmaxf(" + a(0) + ", " + a(1) + ")"); break;
+        case Op::Clamp:
+            f << " { const float lo = " << a(1) << "; return fminf(fmaxf(" << a(0) << ", lo), fmaxf(lo, " << a(2) << ")); }\n";
+            break;
+        case Op::Shift:
+            simple(a(0, "fe_ex(x + " + std::to_string(in.offset[0]) + ")", "fe_ey(y + " + std::to_string(in.offset[1]) + ")",
+                "fe_ez(z + " + std::to_string(in.offset[2]) + ")"));
+            break;
+        case Op::ShiftT:
+            f << " { int lx, hx, ly, hy, lz, hz; fe_run_to(x, " << in.offset[0] << ", NX, lx, hx); fe_run_to(y, " << in.offset[1]
+              << ", NY, ly, hy); fe_run_to(z, " << in.offset[2] << ", NZ, lz, hz);\n"
+              << "    float s = 0.f; for (int k = lz; k <= hz; ++k) for (int j = ly; j <= hy; ++j) for (int i = lx; i <= hx; ++i) s += "
+              << a(0, "i", "j", "k") << ";\n    return s; }\n";
+            break;
+        case Op::GxT: case Op::GyT: case Op::GzT: {
+            const int axis = in.op == Op::GxT ? 0 : (in.op == Op::GyT ? 1 : 2);
+            const char* cc = axis == 0 ? "x" : (axis == 1 ? "y" : "z");
+            const char* n = axis == 0 ? "NX" : (axis == 1 ? "NY" : "NZ");
+            const std::string at_q = axis == 0 ? a(0, "q", "y", "z") : (axis == 1 ? a(0, "x", "q", "z") : a(0, "x", "y", "q"));
+            f << " { float s = 0.f;\n"
+              << "    for (int d = 1; d >= -1; d -= 2) { int lo, hi; fe_run_to(" << cc << ", d, " << n << ", lo, hi);\n"
+              << "        for (int q = lo; q <= hi; ++q) { const int span = fe_imin(q + 1, " << n << " - 1) - fe_imax(q - 1, 0);\n"
+              << "            const float w = span > 0 ? " << at_q << " / (FE_H * span) : 0.f; s += d > 0 ? w : -w; } }\n"
+              << "    return s; }\n";
+            break;
+        }
+        case Op::Lap:
+            f << " { const float c0 = " << a(0) << "; return ((" << a(0, "fe_ex(x - 1)") << " - c0) + (" << a(0, "fe_ex(x + 1)")
+              << " - c0) + (" << a(0, "x", "fe_ey(y - 1)") << " - c0) + (" << a(0, "x", "fe_ey(y + 1)") << " - c0) + ("
+              << a(0, "x", "y", "fe_ez(z - 1)") << " - c0) + (" << a(0, "x", "y", "fe_ez(z + 1)") << " - c0)) / (FE_H * FE_H); }\n";
+            break;
+        case Op::Gx:
+            f << " { const int hi = fe_ex(x + 1); const int lo = fe_ex(x - 1); const int span = hi - lo; return span > 0 ? ("
+              << a(0, "hi") << " - " << a(0, "lo") << ") / (FE_H * span) : 0.f; }\n";
+            break;
+        case Op::Gy:
+            f << " { const int hi = fe_ey(y + 1); const int lo = fe_ey(y - 1); const int span = hi - lo; return span > 0 ? ("
+              << a(0, "x", "hi") << " - " << a(0, "x", "lo") << ") / (FE_H * span) : 0.f; }\n";
+            break;
+        case Op::Gz:
+            f << " { const int hi = fe_ez(z + 1); const int lo = fe_ez(z - 1); const int span = hi - lo; return span > 0 ? ("
+              << a(0, "x", "y", "hi") << " - " << a(0, "x", "y", "lo") << ") / (FE_H * span) : 0.f; }\n";
+            break;
+        case Op::Diffuse: {
+            static const char* sides[6][4] = {{"x > 0", "x - 1", "y", "z"}, {"x + 1 < NX", "x + 1", "y", "z"},
+                {"y > 0", "x", "y - 1", "z"}, {"y + 1 < NY", "x", "y + 1", "z"}, {"z > 0", "x", "y", "z - 1"},
+                {"z + 1 < NZ", "x", "y", "z + 1"}};
+            if (at(in.args[0]).shape == Shape::Scalar) {
+                // One k everywhere: the harmonic mean of a face is k itself (CudaCodegen.cpp:193-206).
+                f << " { const float c0 = " << a(1) << "; float acc = 0.f;\n";
+                for (const auto& s : sides) f << "    if (" << s[0] << ") acc += " << a(1, s[1], s[2], s[3]) << " - c0;\n";
+                f << "    return fmaxf(" << a(0) << ", 0.f) * acc / (FE_H * FE_H); }\n";
+            } else {
+                f << " { const float ka = " << a(0) << "; const float c0 = " << a(1) << "; float acc = 0.f;\n";
+                for (const auto& s : sides) {
+                    f << "    if (" << s[0] << ") acc += fe_face(ka, " << a(0, s[1], s[2], s[3]) << ", c0, " << a(1, s[1], s[2], s[3]) << ");\n";
+                }
+                f << "    return acc / (FE_H * FE_H); }\n";
+            }
+            break;
+        }
+        case Op::Adv: {
+            auto up = [&](const std::string& speed, const char* pos, const char* count, const std::string& lo, const std::string& hi) {
+                return "(" + speed + " > 0.f ? (" + pos + " > 0 ? " + speed + " * (c0 - " + lo + ") / FE_H : 0.f) : (" + pos + " + 1 < " +
+                    count + " ? " + speed + " * (" + hi + " - c0) / FE_H : 0.f))";
+            };
+            f << " { const float c0 = " << a(0) << "; const float u = " << a(1) << "; const float w = " << a(2) << "; const float s = " << a(3)
+              << ";\n    return -(" << up("u", "x", "NX", a(0, "x - 1"), a(0, "x + 1")) << " + "
+              << up("w", "y", "NY", a(0, "x", "y - 1"), a(0, "x", "y + 1")) << " + "
+              << up("s", "z", "NZ", a(0, "x", "y", "z - 1"), a(0, "x", "y", "z + 1")) << "); }\n";
+            break;
+        }
+        case Op::Fall: {
+            const std::string n = std::to_string(id);
+            f << ";\n";
+            f << "template <class C> __device__ __forceinline__ float fall" << n << "(const C& c, int x, int y, int z) { if (z == 0) return 0.f;\n"
+              << "    return fmaxf(0.f, " << a(2) << ") / FE_H * fmaxf(0.f, " << a(0) << ") * fe_sat(1.f - " << a(1, "x", "y", "z - 1")
+              << " - " << a(0, "x", "y", "z - 1") << "); }\n";
+            f << "template <class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)"
+              << " { float o = -fall" << n << "(c, x, y, z); if (z + 1 < NZ) o += fall" << n << "(c, x, y, z + 1); return o; }\n";
+            break;
+        }
+        case Op::Spread: {
+            const std::string n = std::to_string(id);
+            f << ";\n";
+            f << "template <class C> __device__ __forceinline__ float spread" << n << "(const C& c, int ax, int ay, int az, int bx, int by, int bz) {\n"
+              << "    const float fa = " << a(0, "ax", "ay", "az") << "; const float fb = " << a(0, "bx", "by", "bz") << ";\n"
+              << "    const bool to_b = fa > fb; const int rx = to_b ? bx : ax; const int ry = to_b ? by : ay; const int rz = to_b ? bz : az;\n"
+              << "    return 0.5f * (fmaxf(0.f, " << a(2, "ax", "ay", "az") << ") + fmaxf(0.f, " << a(2, "bx", "by", "bz")
+              << ")) / (FE_H * FE_H) * (fa - fb) * fe_sat(1.f - " << a(1, "rx", "ry", "rz") << " - " << a(0, "rx", "ry", "rz") << "); }\n";
+            f << "template <class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)"
+              << " { float o = 0.f;\n"
+              << "    if (y > 0) o += spread" << n << "(c, x, y - 1, z, x, y, z);\n"
+              << "    if (x > 0) o += spread" << n << "(c, x - 1, y, z, x, y, z);\n"
+              << "    if (x + 1 < NX) o -= spread" << n << "(c, x, y, z, x + 1, y, z);\n"
+              << "    if (y + 1 < NY) o -= spread" << n << "(c, x, y, z, x, y + 1, z);\n"
+              << "    return o; }\n";
+            break;
+        }
+        case Op::Topple: {
+            const std::string n = std::to_string(id);
+            f << ";\n";
+            f << "template <class C> __device__ __forceinline__ float room" << n << "(const C& c, int x, int y, int z) { return fe_sat(1.f - " << a(1)
+              << " - " << a(0) << "); }\n"
+              << "template <class C> __device__ __forceinline__ float send" << n << "(const C& c, int x, int y, int z, int sx, int sy) {\n"
+              << "    const float here = " << a(0) << "; if (here <= 0.f || z == 0) return 0.f;\n"
+              << "    if (room" << n << "(c, x, y, z - 1) > 0.01f) return 0.f;\n"
+              << "    const int jx = x + sx; const int jy = y + sy; if (!fe_inside(jx, jy, z)) return 0.f;\n"
+              << "    return 0.25f * fmaxf(0.f, " << a(2) << ") / FE_H * here * fminf(room" << n << "(c, jx, jy, z), room" << n << "(c, jx, jy, z - 1)); }\n";
+            f << "template <class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)"
+              << " { float o = 0.f;\n"
+              << "    o -= send" << n << "(c, x, y, z, -1, 0); o -= send" << n << "(c, x, y, z, 1, 0); o -= send" << n << "(c, x, y, z, 0, -1); o -= send"
+              << n << "(c, x, y, z, 0, 1);\n"
+              << "    if (z + 1 < NZ) {\n"
+              << "        if (x + 1 < NX) o += send" << n << "(c, x + 1, y, z + 1, -1, 0);\n"
+              << "        if (x > 0) o += send" << n << "(c, x - 1, y, z + 1, 1, 0);\n"
+              << "        if (y + 1 < NY) o += send" << n << "(c, x, y + 1, z + 1, 0, -1);\n"
+              << "        if (y > 0) o += send" << n << "(c, x, y - 1, z + 1, 0, 1);\n"
+              << "    }\n    return o; }\n";
+            break;
+        }
+        case Op::Tridiag: case Op::MaxOf: case Op::MinOf: case Op::SumOf:
+            // Only as a body: the stage kernels evaluate their arguments directly.
+            simple("0.f");
+            break;
+        default:
+            simple("0.f");
+            break;
+        }
+    }
+
+    // The pass traits: lattice, tile, sources' layout, outputs' checks.
+    void emit_traits(std::ostringstream& f, const PassBuild& pb, const Launch& L, int nout, const std::vector<char>& checked)
+    {
+        const int nsrc = static_cast<int>(pb.sources.size());
+        f << "struct P {\n"
+          << "    static constexpr int NX = ::NX, NY = ::NY, NZ = ::NZ;\n"
+          << "    static constexpr int W = 8, R = " << L.ty / 8 << ", RZ = " << L.rz << ", NST = " << L.nst << ", NSRC = " << nsrc
+          << ", NOUT = " << nout << ";\n";
+        std::vector<int> ax, ry, px, pl, base;
+        int off = 0;
+        unsigned bytes = 0;
+        for (const Source& s : pb.sources) {
+            const int p_x = 128 + 2 * s.ax;
+            const int p_y = L.ty + 2 * s.ry;
+            const int plane = (p_x * p_y + 31) / 32 * 32;
+            ax.push_back(s.ax);
+            ry.push_back(s.ry);
+            px.push_back(p_x);
+            pl.push_back(plane);
+            base.push_back(off);
+            off += plane * L.nst;
+            bytes += static_cast<unsigned>(p_x * p_y * 4);
+        }
+        auto fn = [&](const char* name, const std::vector<int>& v) {
+            f << "    static __device__ __forceinline__ constexpr int " << name << "(int k) { ";
+            for (std::size_t k = 0; k < v.size(); ++k) f << "if (k == " << k << ") return " << v[k] << "; ";
+            f << "return 0; }\n";
+        };
+        fn("ax", ax);
+        fn("ry", ry);
+        fn("px", px);
+        fn("pl", pl);
+        fn("base", base);
+        f << "    static constexpr unsigned BYTES = " << bytes << "u;\n";
+        f << "    static __device__ __forceinline__ constexpr bool checked(int j) { ";
+        for (int j = 0; j < nout; ++j) f << "if (j == " << j << ") return " << (checked[static_cast<std::size_t>(j)] ? "true" : "false") << "; ";
+        f << "return false; }\n";
+    }
+
+    // Sizes a slab pass's tile and ring to the shared memory; false when no shape fits (the plain twin runs then).
+    bool size_slab(PassBuild& pb, Launch& L)
+    {
+        int rz = 0;
+        for (std::size_t k = 0; k < pb.sources.size(); ++k) {
+            pb.sources[k].ax = (pb.reach[k].x + 3) / 4 * 4;
+            pb.sources[k].ry = pb.reach[k].y;
+            rz = std::max(rz, pb.reach[k].z);
+        }
+        L.rz = rz;
+        if ((nx_ % 4) != 0 || pb.sources.empty() || pb.sources.size() > FE_MAX_SRC_HOST) return false;
+        for (const Source& s : pb.sources) {
+            if (128 + 2 * s.ax > 256 || s.ry > 64) return false;
+        }
+        for (const int ty : {16, 8}) {
+            for (int extra = 2; extra >= 0; --extra) {
+                const int nst = 2 * rz + 2 + extra;
+                std::size_t floats = 0;
+                for (const Source& s : pb.sources) {
+                    const int plane = ((128 + 2 * s.ax) * (ty + 2 * s.ry) + 31) / 32 * 32;
+                    floats += static_cast<std::size_t>(plane) * nst;
+                }
+                if (floats * 4 <= 190 * 1024 && ty + 2 * rz < 256) {
+                    L.ty = ty;
+                    L.nst = nst;
+                    L.smem = static_cast<unsigned>(floats * 4);
+                    return true;
+                }
+            }
+        }
+        return false;
+    }
+
+    static constexpr std::size_t FE_MAX_SRC_HOST = 12;
+    static constexpr std::size_t FE_MAX_OUT_HOST = 8;
+
+    // A pass: computes `outs` (stage bodies, or the gather's targets) at every cell.
+    struct PassOut {
+        enum Kind { StageBody, Gather, Derive } kind = StageBody;
+        int stage = -1;            // StageBody
+        int target = -1;           // Gather / Derive: the field
+        std::vector<int> values;   // Gather: the rates of the equations on the target, in order
+        bool accumulate = false;   // Derive
+        Buf dest;
+    };
+
+    bool emit_pass(const std::string& tag, std::vector<PassOut> outs, Launch& L, std::string& why)
+    {
+        PassBuild pb;
+        std::vector<int> roots;
+        for (const PassOut& o : outs) {
+            if (o.kind == PassOut::StageBody) {
+                pb.own_stages.insert(o.stage);
+                roots.push_back(o.stage);
+            } else {
+                roots.insert(roots.end(), o.values.begin(), o.values.end());
+                // The target's current value at its own cell.
+                source_index(pb, Buf{Buf::FieldNow, o.target});
+            }
+        }
+        const bool bodies = outs.front().kind == PassOut::StageBody;
+        for (const int r : roots) walk(pb, r, Radius{}, bodies);
+        std::ostringstream f;
+        const std::string ns = "fe_" + tag;
+        f << "namespace " << ns << " {\n";
+        emit_functions(f, pb, roots, bodies);
+        if (pb.sources.size() > FE_MAX_SRC_HOST || outs.size() > FE_MAX_OUT_HOST) {
+            why = "a pass of '" + tag + "' reads " + std::to_string(pb.sources.size()) + " buffers and writes " + std::to_string(outs.size()) +
+                " (at most 12 and 8)";
+            return false;
+        }
+        L.kind = Launch::Pass;
+        L.sources = pb.sources;
+        L.slab = size_slab(pb, L);
+        L.sources = pb.sources;
+        std::vector<char> checked;
+        for (const PassOut& o : outs) {
+            L.outs.push_back(o.dest);
+            const bool c = o.kind != PassOut::StageBody;
+            checked.push_back(c ? 1 : 0);
+            L.checked_fields.push_back(c ? o.target : -1);
+        }
+        if (!L.slab) {
+            L.ty = 16;
+            L.nst = 4;
+        }
+        emit_traits(f, pb, L, static_cast<int>(outs.size()), checked);
+        // The cell: every output's value, and the value it replaces (for the contracts).
+        f << "    template <class C> static __device__ __forceinline__ void cell(const C& c, int x, int y, int z, float* o, float* b) {\n";
+        for (std::size_t j = 0; j < outs.size(); ++j) {
+            const PassOut& o = outs[j];
+            if (o.kind == PassOut::StageBody) {
+                f << "        o[" << j << "] = b" << o.stage << "(c, x, y, z); b[" << j << "] = 0.f;\n";
+                continue;
+            }
+            const int k = source_index(pb, Buf{Buf::FieldNow, o.target});
+            if (o.kind == PassOut::Derive) {
+                f << "        { const float v = " << v(o.values[0]) << "; const float old = c.template ld<" << k << ">(x, y, z); b[" << j
+                  << "] = old; o[" << j << "] = " << (o.accumulate ? "old" : "0.f") << " + v; }\n";
+                continue;
+            }
+            f << "        { float n = c.template ld<" << k << ">(x, y, z); b[" << j << "] = n; float d;\n";
+            for (const int val : o.values) {
+                f << "          d = " << v(val) << " * c.dt; if (d != 0.f) n += d;\n";
+            }
+            f << "          o[" << j << "] = n; }\n";
+        }
+        f << "    }\n};\n}\n";
+        L.kernel = "fe_pass_" + tag;
+        L.plain_kernel = "fe_pass_" + tag + "_plain";
+        if (L.slab) {
+            f << "extern \"C\" __global__ void __launch_bounds__(256) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_slab_pass<"
+              << ns << "::P>(a); }\n";
+        }
+        f << "extern \"C\" __global__ void __launch_bounds__(256) " << L.plain_kernel << "(const __grid_constant__ FePassArgs a) { fe_plain_pass<"
+          << ns << "::P>(a); }\n";
+        out_ << f.str();
+        return true;
+    }
+
+    bool emit_tridiag(const std::string& tag, int id, Launch& L, std::string& why)
+    {
+        const Inst& in = at(id);
+        PassBuild pb;
+        for (const int a : in.args) walk(pb, a, Radius{}, false);
+        for (const Radius& r : pb.reach) {
+            if (r.x || r.y || r.z) {
+                why = "a tridiag's coefficients must be read at its own cell";
+                return false;
+            }
+        }
+        std::ostringstream f;
+        const std::string ns = "fe_" + tag;
+        f << "namespace " << ns << " {\n";
+        std::vector<int> roots(in.args.begin(), in.args.end());
+        emit_functions(f, pb, roots, false);
+        L.kind = in.index == 0 ? Launch::TridiagX : Launch::TridiagYZ;
+        L.axis = in.index;
+        L.sources = pb.sources;
+        L.slab = false;
+        L.ty = 16;
+        L.nst = 4;
+        const int slot = plan_.slot_of[static_cast<std::size_t>(id)];
+        L.outs = {Buf{Buf::Slot, slot}, Buf{Buf::Slot, slot + 1}};
+        L.checked_fields = {-1, -1};
+        emit_traits(f, pb, L, 2, {0, 0});
+        f << "    template <class C> static __device__ __forceinline__ void coef(const C& c, int x, int y, int z, float& lo, float& di, float& up, float& rhs) {\n"
+          << "        lo = " << v(in.args[0]) << "; up = " << v(in.args[2]) << "; di = " << v(in.args[1]) << "; rhs = " << v(in.args[3]) << ";\n    }\n";
+        f << "    template <class C> static __device__ __forceinline__ void cell(const C&, int, int, int, float*, float*) {}\n";
+        f << "};\n}\n";
+        L.kernel = "fe_tri_" + tag;
+        if (in.index == 0) {
+            if (nx_ > 640) {
+                why = "tridiag_x keeps a line in shared memory: nx up to 640";
+                return false;
+            }
+            L.smem = static_cast<unsigned>(2 * nx_ * 33 * 4);
+            f << "extern \"C\" __global__ void __launch_bounds__(32) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_tridiag_x_pass<" << ns
+              << "::P>(a); }\n";
+        } else {
+            f << "extern \"C\" __global__ void __launch_bounds__(128) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_tridiag_yz_pass<"
+              << ns << "::P, " << in.index << ">(a); }\n";
+        }
+        out_ << f.str();
+        return true;
+    }
+
+    bool emit_reduce(const std::string& tag, int id, Launch& L)
+    {
+        const Inst& in = at(id);
+        PassBuild pb;
+        walk(pb, in.args[0], Radius{}, false);
+        std::ostringstream f;
+        const std::string ns = "fe_" + tag;
+        f << "namespace " << ns << " {\n";
+        emit_functions(f, pb, {in.args[0]}, false);
+        L.kind = Launch::Reduce;
+        L.sources = pb.sources;
+        L.slab = false;
+        L.uniform = plan_.uniform_of[static_cast<std::size_t>(id)];
+        emit_traits(f, pb, L, 0, {});
+        f << "    static constexpr int KIND = " << (in.op == Op::SumOf ? 0 : (in.op == Op::MaxOf ? 1 : 2)) << ";\n"
+          << "    template <class C> static __device__ __forceinline__ float value(const C& c, int x, int y, int z) { return " << v(in.args[0]) << "; }\n"
+          << "    template <class C> static __device__ __forceinline__ void cell(const C&, int, int, int, float*, float*) {}\n"
+          << "};\n}\n";
+        L.kernel = "fe_red_" + tag;
+        f << "extern \"C\" __global__ void __launch_bounds__(256) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_reduce_pass<" << ns
+          << "::P>(a, &FE_U[" << L.uniform << "]); }\n";
+        out_ << f.str();
+        return true;
+    }
+
+    // Stages in order; consecutive stored stages that do not read one another share a pass.
+    bool emit_stages(const std::string& tag, const std::vector<int>& stages, std::vector<Launch>& launches, std::string& why)
+    {
+        std::vector<int> group;
+        int n = 0;
+        auto flush = [&]() -> bool {
+            if (group.empty()) return true;
+            std::vector<PassOut> outs;
+            for (const int s : group) {
+                PassOut o;
+                o.kind = PassOut::StageBody;
+                o.stage = s;
+                o.dest = Buf{Buf::Slot, plan_.slot_of[static_cast<std::size_t>(s)]};
+                outs.push_back(o);
+            }
+            Launch L;
+            if (!emit_pass(tag + "s" + std::to_string(n++), outs, L, why)) return false;
+            launches.push_back(L);
+            group.clear();
+            return true;
+        };
+        for (const int s : stages) {
+            const Inst& in = at(s);
+            if (in.op == Op::Tridiag || in.global) {
+                if (!flush()) return false;
+                Launch L;
+                if (in.op == Op::Tridiag) {
+                    if (!emit_tridiag(tag + "x" + std::to_string(n++), s, L, why)) return false;
+                } else {
+                    if (!emit_reduce(tag + "r" + std::to_string(n++), s, L)) return false;
+                }
+                launches.push_back(L);
+                continue;
+            }
+            // Does s read (through what it inlines) a stage already in the group?
+            PassBuild probe;
+            probe.own_stages.insert(s);
+            walk(probe, s, Radius{}, true);
+            bool depends = false;
+            for (const Source& src : probe.sources) {
+                for (const int g : group) {
+                    if (src.buf.kind == Buf::Slot && src.buf.id == plan_.slot_of[static_cast<std::size_t>(g)]) depends = true;
+                }
+            }
+            if (depends || group.size() >= FE_MAX_OUT_HOST) {
+                if (!flush()) return false;
+            }
+            group.push_back(s);
+        }
+        return flush();
+    }
+
+    bool program(const ir::Program& p, const std::string& tag, bool derive, ProgramPlan& pp, std::string& why)
+    {
+        pp.empty = p.equations.empty();
+        if (pp.empty) return true;
+        if (!emit_stages(tag, p.stages, pp.stages, why)) return false;
+        if (!emit_stages(tag + "m", p.limit_stages, pp.limit, why)) return false;
+        std::vector<PassOut> outs;
+        if (derive) {
+            const ir::Equation& eq = p.equations[0];
+            const bool reads_itself = std::find(p.reads.begin(), p.reads.end(), eq.target) != p.reads.end();
+            pp.in_place = !reads_itself;
+            PassOut o;
+            o.kind = PassOut::Derive;
+            o.target = eq.target;
+            o.values = {eq.value};
+            o.accumulate = p.accumulate;
+            if (pp.in_place) {
+                o.dest = Buf{Buf::FieldNow, eq.target};
+            } else {
+                o.dest = Buf{Buf::FieldNext, eq.target};
+                pp.swaps.push_back(eq.target);
+                plan_.pingpong[static_cast<std::size_t>(eq.target)] = 1;
+            }
+            outs.push_back(o);
+        } else {
+            pp.in_place = p.in_place;
+            std::vector<int> targets;
+            for (const ir::Equation& eq : p.equations) {
+                if (std::find(targets.begin(), targets.end(), eq.target) == targets.end()) targets.push_back(eq.target);
+            }
+            for (const int t : targets) {
+                PassOut o;
+                o.kind = PassOut::Gather;
+                o.target = t;
+                for (const ir::Equation& eq : p.equations) {
+                    if (eq.target == t) o.values.push_back(eq.value);
+                }
+                if (pp.in_place) {
+                    o.dest = Buf{Buf::FieldNow, t};
+                } else {
+                    o.dest = Buf{Buf::FieldNext, t};
+                    pp.swaps.push_back(t);
+                    plan_.pingpong[static_cast<std::size_t>(t)] = 1;
+                }
+                outs.push_back(o);
+            }
+        }
+        return emit_pass(tag + "g", outs, pp.gather, why);
+    }
+
+    const ir::Module& m_;
+    const law::Law& law_;
+    int nx_, ny_, nz_;
+    double h_;
+    Plan& plan_;
+    std::ostringstream out_;
+};
+
+} // namespace
+
+bool generate(const ir::Module& m, const law::Law& law, int nx, int ny, int nz, double h, Plan& plan, std::string& why)
+{
+    plan = Plan{};
+    Generator g(m, law, nx, ny, nz, h, plan);
+    return g.run(why);
+}
+
+} // namespace fe::gen

@@ -1,0 +1,71 @@
+// IR to CUDA C++ for sm_100a (compiled by NVRTC at run time), and the launch plan the engine follows.
+//
+// What the reference's generator emits (src/field/cuda/CudaCodegen.cpp:300-908) is one thread a cell reading the fields
+// through a ring-addressed constant table; this generator instead emits, per program, passes that march z through
+// TMA-staged slabs of every buffer they read (the skeletons are fe_device.cuh's fe_slab_pass / fe_plain_pass), with the
+// contracts of the term fused into the gather. The per-cell arithmetic is the reference's generated arithmetic, op for
+// op (fp32, no FMA contraction), so a law's step on the card is the same numbers.
+#pragma once
+
+#include "ir.hpp"
+
+#include <string>
+#include <vector>
+
+namespace fe::gen {
+
+// A buffer a launch reads or writes.
+struct Buf {
+    enum Kind : unsigned char { FieldNow, FieldNext, Slot } kind = FieldNow;
+    int id = -1; // field id or slot index
+    bool operator==(const Buf& o) const { return kind == o.kind && id == o.id; }
+};
+
+struct Source {
+    Buf buf;
+    int ax = 0, ry = 0; // staged halo (ax a multiple of 4)
+};
+
+struct Launch {
+    enum Kind : unsigned char { Pass, TridiagX, TridiagYZ, Reduce } kind = Pass;
+    std::string kernel;       // the slab (TMA) kernel, or the only one
+    std::string plain_kernel; // the plain-load twin of a Pass
+    std::vector<Source> sources;
+    std::vector<Buf> outs;
+    std::vector<int> checked_fields; // per out: the field it checks (-1: not a contract output)
+    int ty = 16;              // slab tile rows
+    int nst = 4;              // ring depth
+    int rz = 0;
+    unsigned smem = 0;        // dynamic shared memory of the slab kernel (or the tridiag x kernel)
+    int uniform = -1;         // Reduce: the uniform it writes
+    int axis = 0;
+    bool slab = true;         // the TMA variant is usable
+};
+
+struct ProgramPlan {
+    bool empty = true;
+    std::vector<Launch> stages;       // per substep, in order
+    std::vector<Launch> limit;        // before the substeps (the reductions max_dt reads)
+    Launch gather;
+    std::vector<int> swaps;           // fields whose next buffer becomes now after the gather (ping-pong)
+    bool in_place = false;
+};
+
+struct Plan {
+    int slots = 0;
+    int uniforms = 0;
+    std::vector<int> slot_of;     // per inst: its stored slot (stored stages, tridiag answers), or -1
+    std::vector<int> uniform_of;  // per inst: reductions' uniform, or -1
+    std::vector<char> pingpong;   // per field: has a next buffer
+    std::vector<ProgramPlan> terms, learned, derives;
+    std::string source;           // the translation unit
+};
+
+// Generates the plan and the source for a lattice nx*ny*nz at cell size h. Returns false with `why` when the law uses
+// what this backend does not run.
+bool generate(const ir::Module& m, const law::Law& law, int nx, int ny, int nz, double h, Plan& plan, std::string& why);
+
+// The embedded device prelude (fe_device.cuh).
+const char* device_prelude();
+
+} // namespace fe::gen

@@ -28,6 +28,7 @@ struct Driver {
         void**) = nullptr;
     CUresult (*funcSetAttribute)(CUfunction, CUfunction_attribute, int) = nullptr;
     CUresult (*getErrorString)(CUresult, const char**) = nullptr;
+    CUresult (*moduleGetGlobal)(CUdeviceptr*, size_t*, CUmodule, const char*) = nullptr;
 };
 
 // The driver entry points, looked up once (thread-safe). `ok` is false, with the reason, without a usable driver.

@@ -1,0 +1,773 @@
+#include "engine.hpp"
+
+#include "heat7.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <sstream>
+
+namespace fe {
+
+namespace {
+
+using law::Op;
+
+constexpr int kRing = 64;           // steps of contract records a deferred run may keep on the card
+constexpr int kMaxSubsteps = 4096;  // Solver::kMaxSubsteps (src/field/Solver.hpp:129)
+
+double times(double a, double b)
+{
+    return a == 0.0 || b == 0.0 ? 0.0 : a * b; // 0 * infinity: nothing of it (LawBounds.cpp:8-11)
+}
+
+float key_to_float(unsigned key)
+{
+    const unsigned bits = (key & 0x80000000u) ? (key & 0x7fffffffu) : ~key;
+    float v = 0.0f;
+    std::memcpy(&v, &bits, 4);
+    return v;
+}
+
+std::size_t round256(std::size_t n)
+{
+    return (n + 255) / 256 * 256;
+}
+
+} // namespace
+
+Engine::~Engine()
+{
+    if (stream_ != nullptr) cudaStreamSynchronize(stream_);
+    if (module_ != nullptr && driver().ok) driver().moduleUnload(module_);
+    if (arena_ != nullptr) cudaFree(arena_);
+    if (records_ != nullptr) cudaFree(records_);
+    if (partials_ != nullptr) cudaFree(partials_);
+    if (counts_ != nullptr) cudaFree(counts_);
+    if (ev0_ != nullptr) cudaEventDestroy(ev0_);
+    if (ev1_ != nullptr) cudaEventDestroy(ev1_);
+    if (stream_ != nullptr) cudaStreamDestroy(stream_);
+}
+
+bool Engine::create(const std::vector<law::Source>& sources, int nx, int ny, int nz, double h, std::string& why)
+{
+    if (nx < 1 || ny < 1 || nz < 1 || !(h > 0.0)) {
+        why = "the lattice needs nx, ny, nz >= 1 and h > 0";
+        return false;
+    }
+    if (static_cast<unsigned long long>(nx) * ny * nz >= 0xffffffffull) {
+        why = "more than 2^32 - 1 cells";
+        return false;
+    }
+    nx_ = nx;
+    ny_ = ny;
+    nz_ = nz;
+    h_ = h;
+    cells_ = static_cast<std::size_t>(nx) * ny * nz;
+    std::vector<std::string> errors;
+    law_ = law::compile(sources, errors);
+    if (!errors.empty()) {
+        std::ostringstream all;
+        for (const std::string& e : errors) all << e << "\n";
+        why = all.str();
+        return false;
+    }
+    mod_ = ir::lower(law_);
+    if (!gen::generate(mod_, law_, nx, ny, nz, h, plan_, why)) return false;
+    if (!device_ready(why)) return false;
+    sms_ = sm_count();
+    std::string cubin;
+    std::string log;
+    if (!compile_cubin(plan_.source, "law.cu", cubin, log, &compile_ms_)) {
+        why = "NVRTC could not compile the generated law:\n" + log;
+        return false;
+    }
+    const Driver& d = driver();
+    if (!cu_ok(d.moduleLoadData(&module_, cubin.data()), "cuModuleLoadData", why)) return false;
+    std::size_t bytes = 0;
+    if (!cu_ok(d.moduleGetGlobal(&params_, &bytes, module_, "FE_P"), "FE_P", why)) return false;
+    if (!cu_ok(d.moduleGetGlobal(&uniforms_, &bytes, module_, "FE_U"), "FE_U", why)) return false;
+    if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate", why)) return false;
+    if (!cuda_ok(cudaEventCreate(&ev0_), "cudaEventCreate", why) || !cuda_ok(cudaEventCreate(&ev1_), "cudaEventCreate", why)) return false;
+
+    // One arena: every field's current buffer, the next buffer of the ping-pong ones, every stage slot.
+    const std::size_t field_bytes = round256(cells_ * sizeof(float));
+    const std::size_t fields = law_.fields.size();
+    std::size_t buffers = fields + static_cast<std::size_t>(plan_.slots);
+    for (const char pp : plan_.pingpong) buffers += pp ? 1 : 0;
+    if (!cuda_ok(cudaMalloc(&arena_, std::max<std::size_t>(1, buffers) * field_bytes), "cudaMalloc (lattice)", why)) return false;
+    char* base = static_cast<char*>(arena_);
+    now_.assign(fields, nullptr);
+    next_.assign(fields, nullptr);
+    for (std::size_t f = 0; f < fields; ++f) {
+        now_[f] = reinterpret_cast<float*>(base);
+        base += field_bytes;
+        if (plan_.pingpong[f]) {
+            next_[f] = reinterpret_cast<float*>(base);
+            base += field_bytes;
+        }
+    }
+    for (int s = 0; s < plan_.slots; ++s) {
+        slot_.push_back(reinterpret_cast<float*>(base));
+        base += field_bytes;
+    }
+    bounds_.assign(fields, Bounds{});
+    zero_.assign(fields, 0);
+    for (std::size_t f = 0; f < fields; ++f) {
+        const float init = static_cast<float>(law_.fields[f].init);
+        if (!cuda_ok(launch_fill(now_[f], cells_, init, sms_, stream_), "fill", why)) return false;
+        if (next_[f] != nullptr && !cuda_ok(launch_fill(next_[f], cells_, init, sms_, stream_), "fill", why)) return false;
+        bounds_[f] = Bounds{init, init};
+        zero_[f] = init == 0.0f ? 1 : 0;
+    }
+    for (float* s : slot_) {
+        if (!cuda_ok(cudaMemsetAsync(s, 0, cells_ * sizeof(float), stream_), "memset", why)) return false;
+    }
+
+    // Contract records: one per checked output of every program, per step, in a ring.
+    records_per_step_ = 0;
+    std::size_t partial_doubles = 4 * 1024;
+    auto consider = [&](const gen::Launch& L) {
+        const bool slab = L.slab;
+        const int zchunk = zchunk_for(L, slab);
+        const std::size_t blocks = slab ? static_cast<std::size_t>((nx_ + 127) / 128) * ((ny_ + L.ty - 1) / L.ty) * ((nz_ + zchunk - 1) / zchunk)
+                                        : static_cast<std::size_t>((nx_ + 31) / 32) * ((ny_ + 7) / 8) * ((nz_ + zchunk - 1) / zchunk);
+        const std::size_t plain_blocks = static_cast<std::size_t>((nx_ + 31) / 32) * ((ny_ + 7) / 8) * ((nz_ + zchunk_for(L, false) - 1) / zchunk_for(L, false));
+        partial_doubles = std::max(partial_doubles, 4 * FE_MAX_OUT * std::max(blocks, plain_blocks));
+    };
+    for (const auto* progs : {&plan_.terms, &plan_.learned, &plan_.derives}) {
+        for (const gen::ProgramPlan& pp : *progs) {
+            if (pp.empty) continue;
+            records_per_step_ += static_cast<int>(pp.gather.outs.size());
+            consider(pp.gather);
+            for (const gen::Launch& L : pp.stages) consider(L);
+            for (const gen::Launch& L : pp.limit) consider(L);
+        }
+    }
+    ring_ = kRing;
+    if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&records_), sizeof(FeCheck) * std::max(1, records_per_step_) * ring_), "cudaMalloc (records)", why)) return false;
+    if (!cuda_ok(cudaMemsetAsync(records_, 0, sizeof(FeCheck) * std::max(1, records_per_step_) * ring_, stream_), "memset", why)) return false;
+    partial_doubles_ = partial_doubles;
+    if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&partials_), partial_doubles * sizeof(double)), "cudaMalloc (partials)", why)) return false;
+    if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&counts_), (FE_MAX_OUT + 4) * sizeof(unsigned)), "cudaMalloc (counters)", why)) return false;
+    if (!cuda_ok(cudaMemsetAsync(counts_, 0, (FE_MAX_OUT + 4) * sizeof(unsigned), stream_), "memset", why)) return false;
+
+    param_host_ = law_.param_values;
+    params_dirty_ = true;
+    substeps_.assign(law_.terms.size(), 1);
+    term_profile_.assign(law_.terms.size(), TermProfile{});
+    return cuda_ok(cudaStreamSynchronize(stream_), "create", why);
+}
+
+bool Engine::buffer(const gen::Buf& b, float*& out) const
+{
+    switch (b.kind) {
+    case gen::Buf::FieldNow: out = now_[static_cast<std::size_t>(b.id)]; break;
+    case gen::Buf::FieldNext: out = next_[static_cast<std::size_t>(b.id)]; break;
+    case gen::Buf::Slot: out = slot_[static_cast<std::size_t>(b.id)]; break;
+    }
+    return out != nullptr;
+}
+
+bool Engine::map_for(const float* base, int bx, int by, FeTensorMap& out, std::string& why)
+{
+    const auto key = std::make_tuple(base, bx, by);
+    const auto found = maps_.find(key);
+    if (found != maps_.end()) {
+        out = found->second;
+        return true;
+    }
+    if (!encode_map_3d(&out, base, nx_, ny_, nz_, bx, by, 1, why)) return false;
+    maps_.emplace(key, out);
+    return true;
+}
+
+CUfunction Engine::function(const std::string& name, unsigned smem, std::string& why)
+{
+    const auto found = functions_.find(name);
+    if (found != functions_.end()) return found->second;
+    CUfunction fn = nullptr;
+    if (!cu_ok(driver().moduleGetFunction(&fn, module_, name.c_str()), ("kernel " + name).c_str(), why)) return nullptr;
+    if (smem > 48 * 1024 &&
+        !cu_ok(driver().funcSetAttribute(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, static_cast<int>(smem)), "smem attribute", why)) {
+        return nullptr;
+    }
+    functions_.emplace(name, fn);
+    return fn;
+}
+
+int Engine::zchunk_for(const gen::Launch& L, bool slab) const
+{
+    // Enough CTAs for every SM a few times over; long enough chunks that the z halo is a small part of what is read.
+    const long long tiles = slab ? static_cast<long long>((nx_ + 127) / 128) * ((ny_ + L.ty - 1) / L.ty)
+                                 : static_cast<long long>((nx_ + 31) / 32) * ((ny_ + 7) / 8);
+    const long long want = static_cast<long long>(sms_) * (slab ? 3 : 6);
+    const long long chunks = std::max<long long>(1, (want + tiles - 1) / tiles);
+    int zchunk = static_cast<int>((nz_ + chunks - 1) / chunks);
+    if (L.rz > 0) zchunk = std::max(zchunk, std::min(nz_, 16 * L.rz));
+    return std::max(1, zchunk);
+}
+
+bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* recs, std::string& why)
+{
+    FePassArgs a;
+    std::memset(&a, 0, sizeof(a));
+    const bool slab = L.kind == gen::Launch::Pass && L.slab;
+    for (std::size_t k = 0; k < L.sources.size(); ++k) {
+        float* p = nullptr;
+        if (!buffer(L.sources[k].buf, p)) {
+            why = "internal: a pass reads a buffer that does not exist";
+            return false;
+        }
+        a.src[k] = p;
+        if (slab && !map_for(p, 128 + 2 * L.sources[k].ax, L.ty + 2 * L.sources[k].ry, a.map[k], why)) return false;
+    }
+    for (std::size_t j = 0; j < L.outs.size(); ++j) {
+        if (!buffer(L.outs[j], a.out[j])) {
+            why = "internal: a pass writes a buffer that does not exist";
+            return false;
+        }
+        const int f = j < L.checked_fields.size() ? L.checked_fields[j] : -1;
+        a.rec[j] = (recs != nullptr && f >= 0) ? recs[j] : nullptr;
+        a.lo[j] = f >= 0 ? static_cast<float>(law_.fields[static_cast<std::size_t>(f)].lo) : -3.0e38f;
+        a.hi[j] = f >= 0 ? static_cast<float>(law_.fields[static_cast<std::size_t>(f)].hi) : 3.0e38f;
+    }
+    a.partials = partials_;
+    a.count = counts_;
+    a.err = counts_ + FE_MAX_OUT;
+    a.dt = dt;
+    a.flags = flags;
+    void* params[] = {&a};
+    unsigned gx = 1, gy = 1, gz = 1, block = 256, smem = 0;
+    std::string name = L.kernel;
+    switch (L.kind) {
+    case gen::Launch::Pass: {
+        const int zchunk = zchunk_for(L, slab);
+        a.zchunk = zchunk;
+        if (slab) {
+            gx = static_cast<unsigned>((nx_ + 127) / 128);
+            gy = static_cast<unsigned>((ny_ + L.ty - 1) / L.ty);
+            smem = L.smem;
+        } else {
+            name = L.plain_kernel;
+            gx = static_cast<unsigned>((nx_ + 31) / 32);
+            gy = static_cast<unsigned>((ny_ + 7) / 8);
+        }
+        gz = static_cast<unsigned>((nz_ + zchunk - 1) / zchunk);
+        break;
+    }
+    case gen::Launch::TridiagX:
+        gx = static_cast<unsigned>((ny_ + 31) / 32);
+        gy = static_cast<unsigned>(nz_);
+        block = 32;
+        smem = L.smem;
+        break;
+    case gen::Launch::TridiagYZ: {
+        const unsigned long long lines = L.axis == 1 ? static_cast<unsigned long long>(nx_) * nz_ : static_cast<unsigned long long>(nx_) * ny_;
+        block = 128;
+        gx = static_cast<unsigned>((lines + 127) / 128);
+        break;
+    }
+    case gen::Launch::Reduce:
+        block = 256;
+        gx = static_cast<unsigned>(std::min<std::size_t>((cells_ + 255) / 256, static_cast<std::size_t>(sms_) * 4));
+        break;
+    }
+    a.blocks = static_cast<int>(gx * gy * gz);
+    if (static_cast<std::size_t>(a.blocks) * 4 * FE_MAX_OUT > partial_doubles_) {
+        why = "internal: too few partial sums for a launch";
+        return false;
+    }
+    CUfunction fn = function(name, smem, why);
+    if (fn == nullptr) return false;
+    ++launches_;
+    return cu_ok(driver().launchKernel(fn, gx, gy, gz, block, 1, 1, smem, reinterpret_cast<CUstream>(stream_), params, nullptr),
+        ("launch " + name).c_str(), why);
+}
+
+bool Engine::set_param(int id, double value)
+{
+    if (id < 0 || static_cast<std::size_t>(id) >= param_host_.size()) return false;
+    param_host_[static_cast<std::size_t>(id)] = value;
+    law_.param_values[static_cast<std::size_t>(id)] = value;
+    params_dirty_ = true;
+    return true;
+}
+
+bool Engine::upload(int field, const void* src, bool device, std::string& why)
+{
+    if (field < 0 || static_cast<std::size_t>(field) >= now_.size()) {
+        why = "no field " + std::to_string(field);
+        return false;
+    }
+    if (!sync(why)) return false;
+    const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    if (!cuda_ok(cudaMemcpyAsync(now_[static_cast<std::size_t>(field)], src, cells_ * sizeof(float), kind, stream_), "upload", why)) return false;
+    if (!cuda_ok(cudaStreamSynchronize(stream_), "upload", why)) return false;
+    Bounds b{std::numeric_limits<double>::infinity(), -std::numeric_limits<double>::infinity()};
+    if (!device) {
+        // What the host writes it has at hand: its bounds, for the idle-term test (CudaSolver.cpp:820-920 looks over
+        // uploaded planes the same way).
+        const float* v = static_cast<const float*>(src);
+        float lo = std::numeric_limits<float>::infinity(), hi = -lo;
+        for (std::size_t i = 0; i < cells_; ++i) {
+            const float x = v[i];
+            if (x != x) continue;
+            lo = std::min(lo, x);
+            hi = std::max(hi, x);
+        }
+        b = Bounds{lo, hi};
+        if (lo > hi) b = Bounds{};
+    } else {
+        b = Bounds{};
+    }
+    bounds_[static_cast<std::size_t>(field)] = b;
+    zero_[static_cast<std::size_t>(field)] = (b.lo == 0.0 && b.hi == 0.0) ? 1 : 0;
+    return true;
+}
+
+bool Engine::fetch(int field, void* dst, bool device, std::string& why)
+{
+    if (field < 0 || static_cast<std::size_t>(field) >= now_.size()) {
+        why = "no field " + std::to_string(field);
+        return false;
+    }
+    const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (!cuda_ok(cudaMemcpyAsync(dst, now_[static_cast<std::size_t>(field)], cells_ * sizeof(float), kind, stream_), "fetch", why)) return false;
+    return cuda_ok(cudaStreamSynchronize(stream_), "fetch", why);
+}
+
+// ---- the idle-term test (LawBounds.cpp:13-213 over the IR) ---------------------------------------------------------------
+
+Bounds Engine::bounds_of(int id, const std::vector<Bounds>& fields) const
+{
+    const ir::Inst& in = mod_.insts[static_cast<std::size_t>(id)];
+    auto arg = [&](std::size_t i) { return bounds_of(in.args[i], fields); };
+    auto clean = [](double lo, double hi) {
+        return Bounds{std::isnan(lo) ? -std::numeric_limits<double>::infinity() : lo, std::isnan(hi) ? std::numeric_limits<double>::infinity() : hi};
+    };
+    auto spread = [](const Bounds& b) { return b.lo == b.hi ? 0.0 : b.hi - b.lo; };
+    switch (in.op) {
+    case Op::Const: return Bounds{in.number, in.number};
+    case Op::Param: {
+        const double v = static_cast<float>(law_.param_values[static_cast<std::size_t>(in.index)]);
+        return Bounds{v, v};
+    }
+    case Op::Cell: return Bounds{h_, h_};
+    case Op::Rim: return Bounds{0.0, 1.0};
+    case Op::Field: return fields[static_cast<std::size_t>(in.index)];
+    case Op::Neg: { const Bounds a = arg(0); return Bounds{-a.hi, -a.lo}; }
+    case Op::Add: { const Bounds a = arg(0), b = arg(1); return clean(a.lo + b.lo, a.hi + b.hi); }
+    case Op::Sub: { const Bounds a = arg(0), b = arg(1); return clean(a.lo - b.hi, a.hi - b.lo); }
+    case Op::Mul: {
+        const Bounds a = arg(0), b = arg(1);
+        const double c[4] = {times(a.lo, b.lo), times(a.lo, b.hi), times(a.hi, b.lo), times(a.hi, b.hi)};
+        return Bounds{*std::min_element(c, c + 4), *std::max_element(c, c + 4)};
+    }
+    case Op::Div: {
+        const Bounds a = arg(0), b = arg(1);
+        if (a.none() || b.none()) return Bounds{0.0, 0.0};
+        if (b.lo <= 0.0 && b.hi >= 0.0) return Bounds{};
+        const double c[4] = {a.lo / b.lo, a.lo / b.hi, a.hi / b.lo, a.hi / b.hi};
+        return clean(*std::min_element(c, c + 4), *std::max_element(c, c + 4));
+    }
+    case Op::Pow: {
+        const Bounds a = arg(0), b = arg(1);
+        if (a.none() && b.lo > 0.0) return Bounds{0.0, 0.0};
+        if (a.lo >= 0.0 && b.lo == b.hi && b.lo > 0.0) return clean(std::pow(a.lo, b.lo), std::pow(a.hi, b.lo));
+        return Bounds{};
+    }
+    case Op::Min: { const Bounds a = arg(0), b = arg(1); return Bounds{std::min(a.lo, b.lo), std::min(a.hi, b.hi)}; }
+    case Op::Max: { const Bounds a = arg(0), b = arg(1); return Bounds{std::max(a.lo, b.lo), std::max(a.hi, b.hi)}; }
+    case Op::Abs: {
+        const Bounds a = arg(0);
+        const double most = std::max(std::abs(a.lo), std::abs(a.hi));
+        return Bounds{a.lo <= 0.0 && a.hi >= 0.0 ? 0.0 : std::min(std::abs(a.lo), std::abs(a.hi)), most};
+    }
+    case Op::Sqrt: { const Bounds a = arg(0); return Bounds{std::sqrt(std::max(0.0, a.lo)), std::sqrt(std::max(0.0, a.hi))}; }
+    case Op::Exp: { const Bounds a = arg(0); return Bounds{std::exp(std::min(a.lo, 80.0)), std::exp(std::min(a.hi, 80.0))}; }
+    case Op::Log: { const Bounds a = arg(0); return Bounds{std::log(std::max(a.lo, 1e-30)), std::log(std::max(a.hi, 1e-30))}; }
+    case Op::Step: { const Bounds a = arg(0); return Bounds{a.lo > 0.0 ? 1.0 : 0.0, a.hi > 0.0 ? 1.0 : 0.0}; }
+    case Op::Pos: { const Bounds a = arg(0); return Bounds{std::max(a.lo, 0.0), std::max(a.hi, 0.0)}; }
+    case Op::Clamp: {
+        const Bounds a = arg(0), lo = arg(1), hi = arg(2);
+        return Bounds{std::min(std::max(a.lo, lo.lo), std::max(lo.hi, hi.hi)), std::min(std::max(a.hi, lo.hi), std::max(lo.hi, hi.hi))};
+    }
+    case Op::Shift: case Op::MaxOf: case Op::MinOf: return arg(0);
+    case Op::Lap: { const double most = 6.0 * spread(arg(0)) / (h_ * h_); return Bounds{-most, most}; }
+    case Op::Gx: case Op::Gy: case Op::Gz: { const double most = spread(arg(0)) / h_; return Bounds{-most, most}; }
+    case Op::Diffuse: {
+        const Bounds k = arg(0);
+        const double most = times(12.0 * std::max(std::abs(k.lo), std::abs(k.hi)), spread(arg(1))) / (h_ * h_);
+        return Bounds{-most, most};
+    }
+    case Op::Adv: case Op::Fall: case Op::Spread: case Op::Topple: case Op::SumOf: {
+        const Bounds a = arg(0);
+        return a.none() ? a : Bounds{};
+    }
+    default:
+        return Bounds{};
+    }
+}
+
+bool Engine::always_zero(int id) const
+{
+    const ir::Inst& in = mod_.insts[static_cast<std::size_t>(id)];
+    auto arg = [&](std::size_t i) { return always_zero(in.args[i]); };
+    switch (in.op) {
+    case Op::Const: return in.number == 0.0;
+    case Op::Param: return law_.param_values[static_cast<std::size_t>(in.index)] == 0.0;
+    case Op::Field: return zero_[static_cast<std::size_t>(in.index)] != 0;
+    case Op::Neg: case Op::Abs: case Op::Sqrt: case Op::Step: case Op::Pos: case Op::Shift: case Op::Lap: case Op::Gx: case Op::Gy:
+    case Op::Gz: case Op::MaxOf: case Op::MinOf: case Op::SumOf:
+        return arg(0);
+    case Op::Mul: case Op::Div: return arg(0) || arg(1);
+    case Op::Add: case Op::Sub: case Op::Min: case Op::Max: return arg(0) && arg(1);
+    case Op::Diffuse: return arg(0) || arg(1);
+    case Op::Adv: case Op::Fall: case Op::Spread: case Op::Topple: return arg(0);
+    default: return false;
+    }
+}
+
+bool Engine::idle(const ir::Program& p) const
+{
+    return std::all_of(p.equations.begin(), p.equations.end(),
+        [&](const ir::Equation& eq) { return always_zero(eq.value) || bounds_of(eq.value, bounds_).none(); });
+}
+
+// What a term of `substeps` Euler substeps may have done to the bounds of what it writes (LawBounds.cpp:219-268).
+void Engine::flow_bounds(const ir::Program& p, double dt, int substeps)
+{
+    const int n = std::max(substeps, 1);
+    const double sub = dt / n;
+    const std::vector<Bounds> before = bounds_;
+    for (int s = 0; s < n; ++s) {
+        const std::vector<Bounds> start = bounds_;
+        std::vector<Bounds> now = bounds_;
+        for (int round = 0; round < 2; ++round) {
+            std::vector<Bounds> next = now;
+            for (const ir::Equation& eq : p.equations) {
+                const ir::Inst& in = mod_.insts[static_cast<std::size_t>(eq.value)];
+                const bool within = in.op == Op::Diffuse && mod_.insts[static_cast<std::size_t>(in.args[1])].op == Op::Field &&
+                    mod_.insts[static_cast<std::size_t>(in.args[1])].index == eq.target;
+                if (within) continue;
+                const auto t = static_cast<std::size_t>(eq.target);
+                const Bounds rate = bounds_of(eq.value, now);
+                next[t].lo = std::min(next[t].lo, start[t].lo + times(sub, std::min(rate.lo, 0.0)));
+                next[t].hi = std::max(next[t].hi, start[t].hi + times(sub, std::max(rate.hi, 0.0)));
+            }
+            now = std::move(next);
+        }
+        bool moved = false;
+        for (std::size_t f = 0; f < now.size() && !moved; ++f) moved = now[f].lo != bounds_[f].lo || now[f].hi != bounds_[f].hi;
+        bounds_ = std::move(now);
+        if (!moved) break;
+    }
+    for (const ir::Equation& eq : p.equations) {
+        const auto t = static_cast<std::size_t>(eq.target);
+        const law::FieldDecl& decl = law_.fields[t];
+        Bounds& b = bounds_[t];
+        if (b.lo != before[t].lo || b.hi != before[t].hi) {
+            b.lo -= 1e-6 * n * std::abs(b.lo);
+            b.hi += 1e-6 * n * std::abs(b.hi);
+        }
+        if (decl.clamp) {
+            b.lo = std::clamp(b.lo, decl.lo, decl.hi);
+            b.hi = std::clamp(b.hi, decl.lo, decl.hi);
+        }
+        zero_[t] = (b.lo == 0.0 && b.hi == 0.0) ? 1 : 0;
+    }
+}
+
+// A max_dt on the host: numbers, params, h, and reductions read back from the card (CudaSolver.cpp:450-488).
+double Engine::scalar_value(int id, bool& ok, std::string& why)
+{
+    const ir::Inst& in = mod_.insts[static_cast<std::size_t>(id)];
+    auto a = [&](std::size_t k) { return scalar_value(in.args[k], ok, why); };
+    switch (in.op) {
+    case Op::Const: return in.number;
+    case Op::Param: return law_.param_values[static_cast<std::size_t>(in.index)];
+    case Op::Cell: return h_;
+    case Op::Neg: return -a(0);
+    case Op::Abs: return std::abs(a(0));
+    case Op::Sqrt: return std::sqrt(std::max(0.0, a(0)));
+    case Op::Exp: return std::exp(std::min(a(0), 80.0));
+    case Op::Log: return std::log(std::max(a(0), 1e-30));
+    case Op::Step: return a(0) > 0.0 ? 1.0 : 0.0;
+    case Op::Pos: return std::max(a(0), 0.0);
+    case Op::Add: return a(0) + a(1);
+    case Op::Sub: return a(0) - a(1);
+    case Op::Mul: return a(0) * a(1);
+    case Op::Div: { const double b = a(1); return b == 0.0 ? 0.0 : a(0) / b; }
+    case Op::Pow: return std::pow(a(0), a(1));
+    case Op::Min: return std::min(a(0), a(1));
+    case Op::Max: return std::max(a(0), a(1));
+    case Op::Clamp: { const double lo = a(1); return std::clamp(a(0), lo, std::max(lo, a(2))); }
+    case Op::MaxOf: case Op::MinOf: case Op::SumOf: {
+        const int u = plan_.uniform_of[static_cast<std::size_t>(id)];
+        if (u < 0) return 0.0;
+        float value = 0.0f;
+        if (!cuda_ok(cudaMemcpyAsync(&value, reinterpret_cast<const char*>(uniforms_) + 4 * u, 4, cudaMemcpyDeviceToHost, stream_), "uniform", why) ||
+            !cuda_ok(cudaStreamSynchronize(stream_), "uniform", why)) {
+            ok = false;
+        }
+        return value;
+    }
+    default:
+        return 0.0;
+    }
+}
+
+bool Engine::run_program(int index, const ir::Program& p, const gen::ProgramPlan& pp, double dt, bool respect, bool check,
+    PendingStep& pending, std::string& why)
+{
+    TermProfile& tp = term_profile_[static_cast<std::size_t>(index)];
+    tp = TermProfile{};
+    const int launches_before = launches_;
+    substeps_[static_cast<std::size_t>(index)] = 1;
+    if (pp.empty) return true;
+    if (idle(p)) {
+        tp.idle = true;
+        return true;
+    }
+    int count = 1;
+    if (respect && p.max_dt >= 0) {
+        for (const gen::Launch& L : pp.limit) {
+            if (!launch(L, 0.0f, 0, nullptr, why)) return false;
+        }
+        bool ok = true;
+        const double limit = scalar_value(p.max_dt, ok, why);
+        if (!ok) return false;
+        if (limit > 0.0 && std::isfinite(limit) && dt > limit) {
+            const double wanted = std::ceil(dt / limit);
+            if (wanted > kMaxSubsteps) {
+                Violation v;
+                v.kind = 3;
+                v.term = index;
+                v.step = steps_;
+                v.detail = "max_dt " + std::to_string(limit) + " asks for " + std::to_string(wanted) + " substeps; capped at " +
+                    std::to_string(kMaxSubsteps);
+                violations_.push_back(v);
+                count = kMaxSubsteps;
+            } else {
+                count = static_cast<int>(wanted);
+            }
+        }
+    }
+    substeps_[static_cast<std::size_t>(index)] = count;
+    const float sub_dt = static_cast<float>(dt / count);
+    FeCheck* recs[FE_MAX_OUT] = {};
+    if (check) {
+        for (std::size_t j = 0; j < pp.gather.outs.size(); ++j) {
+            const int r = static_cast<int>(pending.refs.size());
+            recs[j] = records_ + static_cast<std::size_t>(pending.ring) * records_per_step_ + r;
+            pending.refs.push_back(RecordRef{index, pp.gather.checked_fields[j], r, count, true});
+        }
+    }
+    for (int s = 0; s < count; ++s) {
+        for (const gen::Launch& L : pp.stages) {
+            if (!launch(L, sub_dt, 0, nullptr, why)) return false;
+        }
+        int flags = 0;
+        if (s == 0) flags |= FE_PASS_BEFORE;
+        if (s == count - 1) flags |= FE_PASS_AFTER | FE_PASS_RANGE;
+        if (!launch(pp.gather, sub_dt, flags, check ? recs : nullptr, why)) return false;
+        for (const int f : pp.swaps) std::swap(now_[static_cast<std::size_t>(f)], next_[static_cast<std::size_t>(f)]);
+    }
+    flow_bounds(p, dt, count);
+    tp.launches = launches_ - launches_before;
+    tp.substeps = count;
+    return true;
+}
+
+bool Engine::step(double dt, bool respect_max_dt, std::string& why)
+{
+    if (!deferred_) violations_.clear();
+    launches_ = 0;
+    if (params_dirty_) {
+        std::vector<float> p(1024, 0.0f);
+        for (std::size_t i = 0; i < param_host_.size() && i < 1024; ++i) p[i] = static_cast<float>(param_host_[i]);
+        if (!cuda_ok(cudaMemcpyAsync(reinterpret_cast<void*>(params_), p.data(), 1024 * sizeof(float), cudaMemcpyHostToDevice, stream_), "params", why) ||
+            !cuda_ok(cudaStreamSynchronize(stream_), "params", why)) {
+            return false;
+        }
+        params_dirty_ = false;
+    }
+    const bool check = (steps_ % check_every_) == 0;
+    PendingStep pending;
+    pending.step = steps_;
+    pending.ring = ring_next_;
+    if (check) {
+        ring_next_ = (ring_next_ + 1) % ring_;
+        if (records_per_step_ > 0 &&
+            !cuda_ok(cudaMemsetAsync(records_ + static_cast<std::size_t>(pending.ring) * records_per_step_, 0, sizeof(FeCheck) * records_per_step_, stream_),
+                "records", why)) {
+            return false;
+        }
+    }
+    cudaEventRecord(ev0_, stream_);
+    for (std::size_t t = 0; t < mod_.terms.size(); ++t) {
+        if (!run_program(static_cast<int>(t), mod_.terms[t], plan_.terms[t], dt, respect_max_dt, check, pending, why)) return false;
+    }
+    for (std::size_t d = 0; d < mod_.derives.size(); ++d) {
+        const gen::ProgramPlan& pp = plan_.derives[d];
+        if (pp.empty) continue;
+        FeCheck* recs[FE_MAX_OUT] = {};
+        if (check) {
+            const int r = static_cast<int>(pending.refs.size());
+            recs[0] = records_ + static_cast<std::size_t>(pending.ring) * records_per_step_ + r;
+            pending.refs.push_back(RecordRef{-1, pp.gather.checked_fields[0], r, 1, false});
+        }
+        for (const gen::Launch& L : pp.stages) {
+            if (!launch(L, 0.0f, 0, nullptr, why)) return false;
+        }
+        if (!launch(pp.gather, 0.0f, FE_PASS_RANGE, check ? recs : nullptr, why)) return false;
+        for (const int f : pp.swaps) std::swap(now_[static_cast<std::size_t>(f)], next_[static_cast<std::size_t>(f)]);
+    }
+    cudaEventRecord(ev1_, stream_);
+    ++steps_;
+    gpu_ms_ = 0.0;
+    if (!check) return cuda_ok(cudaPeekAtLastError(), "step", why);
+    pending_.push_back(std::move(pending));
+    if (!deferred_ || static_cast<int>(pending_.size()) >= ring_ - 1) {
+        if (!sync(why)) return false;
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, ev0_, ev1_) == cudaSuccess) gpu_ms_ = ms;
+    }
+    return true;
+}
+
+bool Engine::derive(std::string& why)
+{
+    for (std::size_t d = 0; d < mod_.derives.size(); ++d) {
+        const gen::ProgramPlan& pp = plan_.derives[d];
+        if (pp.empty) continue;
+        for (const gen::Launch& L : pp.stages) {
+            if (!launch(L, 0.0f, 0, nullptr, why)) return false;
+        }
+        if (!launch(pp.gather, 0.0f, 0, nullptr, why)) return false;
+        for (const int f : pp.swaps) std::swap(now_[static_cast<std::size_t>(f)], next_[static_cast<std::size_t>(f)]);
+    }
+    return cuda_ok(cudaStreamSynchronize(stream_), "derive", why);
+}
+
+bool Engine::sync(std::string& why)
+{
+    if (!cuda_ok(cudaStreamSynchronize(stream_), "sync", why)) return false;
+    unsigned err = 0;
+    if (!cuda_ok(cudaMemcpy(&err, counts_ + FE_MAX_OUT, 4, cudaMemcpyDeviceToHost), "error word", why)) return false;
+    if (err != 0) {
+        why = "a kernel raised error word " + std::to_string(err) + " (a bounded wait gave up)";
+        return false;
+    }
+    for (std::size_t i = 0; i < pending_.size(); ++i) {
+        if (!judge(pending_[i], why)) return false;
+        if (i + 1 == pending_.size()) {
+            // The latest step's records are the fields' exact bounds now.
+            std::vector<FeCheck> recs(static_cast<std::size_t>(std::max(1, records_per_step_)));
+            cudaMemcpy(recs.data(), records_ + static_cast<std::size_t>(pending_[i].ring) * records_per_step_, sizeof(FeCheck) * records_per_step_,
+                cudaMemcpyDeviceToHost);
+            for (const RecordRef& r : pending_[i].refs) {
+                const FeCheck& c = recs[static_cast<std::size_t>(r.rec)];
+                if (r.field < 0) continue;
+                const unsigned lo_key = ~c.lo_inv;
+                if (c.hi_key != 0u && lo_key != 0xffffffffu) {
+                    bounds_[static_cast<std::size_t>(r.field)] = Bounds{key_to_float(lo_key), key_to_float(c.hi_key)};
+                    zero_[static_cast<std::size_t>(r.field)] = (key_to_float(lo_key) == 0.0f && key_to_float(c.hi_key) == 0.0f) ? 1 : 0;
+                }
+            }
+        }
+    }
+    pending_.clear();
+    return true;
+}
+
+// The host's judgement of one step's records (CudaSolver.cpp:530-571; the tolerance is Solver.cpp:439-453's).
+bool Engine::judge(PendingStep& pending, std::string& why)
+{
+    if (pending.refs.empty()) return true;
+    std::vector<FeCheck> recs(static_cast<std::size_t>(records_per_step_));
+    if (!cuda_ok(cudaMemcpy(recs.data(), records_ + static_cast<std::size_t>(pending.ring) * records_per_step_, sizeof(FeCheck) * records_per_step_,
+                     cudaMemcpyDeviceToHost),
+            "records", why)) {
+        return false;
+    }
+    // Conservation, per term and group.
+    for (std::size_t t = 0; t < law_.terms.size(); ++t) {
+        const law::Term& term = law_.terms[t];
+        for (const std::vector<int>& group : term.conserves) {
+            double before = 0.0, after = 0.0, scale = 0.0;
+            int substeps = 1;
+            bool any = false;
+            for (const int f : group) {
+                for (const RecordRef& r : pending.refs) {
+                    if (r.term == static_cast<int>(t) && r.field == f) {
+                        const FeCheck& c = recs[static_cast<std::size_t>(r.rec)];
+                        before += c.before;
+                        after += c.after;
+                        scale += c.before_abs;
+                        substeps = r.substeps;
+                        any = true;
+                    }
+                }
+            }
+            if (!any) continue; // the term was idle: nothing moved
+            const double tolerance = 1e-5 * (scale + 1.0) * std::sqrt(static_cast<double>(substeps));
+            if (std::abs(after - before) > tolerance) {
+                Violation v;
+                v.kind = 2;
+                v.term = static_cast<int>(t);
+                v.field = group.front();
+                v.before = before;
+                v.after = after;
+                v.tolerance = tolerance;
+                v.step = pending.step;
+                std::ostringstream d;
+                d << "total went " << before << " -> " << after << " (tolerance " << tolerance << ")";
+                v.detail = d.str();
+                violations_.push_back(v);
+            }
+        }
+    }
+    // Range and NaN, per written field.
+    for (const RecordRef& r : pending.refs) {
+        const FeCheck& c = recs[static_cast<std::size_t>(r.rec)];
+        if (c.out_of_range == 0 && c.not_finite == 0) continue;
+        Violation v;
+        v.kind = c.not_finite != 0 ? 1 : 0;
+        v.term = r.term;
+        v.field = r.field;
+        v.count = c.out_of_range + c.not_finite;
+        v.first_cell = ~c.first_bad;
+        v.step = pending.step;
+        const law::FieldDecl& decl = law_.fields[static_cast<std::size_t>(r.field)];
+        const unsigned first = v.first_cell;
+        std::ostringstream d;
+        d << v.count << " cell(s); first " << decl.name << " at (" << first % nx_ << "," << (first / nx_) % ny_ << "," << first / (static_cast<unsigned>(nx_) * ny_)
+          << "), declared range [" << decl.lo << ", " << decl.hi << "]";
+        v.detail = d.str();
+        violations_.push_back(v);
+    }
+    return true;
+}
+
+bool Engine::time_gather(int term, int launches, float& ms, std::string& why)
+{
+    if (term < 0 || static_cast<std::size_t>(term) >= plan_.terms.size() || plan_.terms[static_cast<std::size_t>(term)].empty) {
+        why = "no such term";
+        return false;
+    }
+    const gen::ProgramPlan& pp = plan_.terms[static_cast<std::size_t>(term)];
+    FeCheck* recs[FE_MAX_OUT] = {};
+    for (std::size_t j = 0; j < pp.gather.outs.size(); ++j) recs[j] = records_ + j; // scratch records (ring slot 0)
+    cudaEventRecord(ev0_, stream_);
+    for (int i = 0; i < launches; ++i) {
+        if (!launch(pp.gather, static_cast<float>(0.0), FE_PASS_BEFORE | FE_PASS_AFTER | FE_PASS_RANGE, recs, why)) return false;
+    }
+    cudaEventRecord(ev1_, stream_);
+    if (!cuda_ok(cudaEventSynchronize(ev1_), "time", why)) return false;
+    return cuda_ok(cudaEventElapsedTime(&ms, ev0_, ev1_), "time", why);
+}
+
+} // namespace fe

@@ -34,6 +34,30 @@ struct FeCheck {
 // Error words a kernel raises instead of hanging or trapping (bounded waits).
 #define FE_ERR_MBAR_TIMEOUT 1u
 
+// The one parameter block of every generated pass kernel (a fused gather, or a group of stored stages): the host fills
+// it, the kernel reads it as a __grid_constant__. Sources are the buffers the pass reads (a field's current buffer or a
+// stage's slot), each with its TMA map; outputs are the buffers it writes, each optionally with a contract record.
+#define FE_MAX_SRC 12
+#define FE_MAX_OUT 8
+struct FePassArgs {
+    FeTensorMap map[FE_MAX_SRC];
+    const float* src[FE_MAX_SRC];
+    float* out[FE_MAX_OUT];
+    FeCheck* rec[FE_MAX_OUT];  // null: this output is not checked in this pass
+    float lo[FE_MAX_OUT];      // declared range of a checked output's field
+    float hi[FE_MAX_OUT];
+    double* partials;          // [FE_MAX_OUT][blocks][4]
+    unsigned* count;           // [FE_MAX_OUT] blocks finished
+    unsigned* err;
+    float dt;
+    int flags;                 // FE_PASS_BEFORE | FE_PASS_AFTER
+    int zchunk;
+    int blocks;
+};
+#define FE_PASS_BEFORE 1  // record the totals before the pass (the term's first substep)
+#define FE_PASS_AFTER 2   // record the totals after the pass (the term's last substep)
+#define FE_PASS_RANGE 4   // record range/NaN counts and bounds of what the pass writes (the term's last substep)
+
 // Everything below is device code (nvcc's device pass or NVRTC); host translation units see only the types above.
 #if defined(__CUDACC__) || defined(__CUDACC_RTC__)
 
@@ -142,40 +166,75 @@ __device__ __forceinline__ unsigned fe_warp_max(unsigned v)
     return v;
 }
 
-// Per-thread contract accumulators of one checked field in a gather pass.
+// Per-thread contract accumulators of one checked field in a gather pass. Totals are FP64; each group of 4 cells a lane
+// owns is first summed in fp32 ((c0 + c1) + (c2 + c3)), whose rounding (a few 1e-8 of the group) is far below the
+// conservation tolerance (1e-5 of the total of |field|). Bounds are float min/max (NaN ignored), turned into ordered
+// keys once per block.
 struct FeAcc {
     double before, before_abs, after, after_abs;
-    unsigned lo, hi, bad, nan, first, changed;
+    float lo, hi;
+    unsigned bad, nan, first, changed;
 };
 
 __device__ __forceinline__ void fe_acc_init(FeAcc& a)
 {
     a.before = 0.0; a.before_abs = 0.0; a.after = 0.0; a.after_abs = 0.0;
-    a.lo = 0xffffffffu; a.hi = 0u; a.bad = 0u; a.nan = 0u; a.first = 0u; a.changed = 0u;
+    a.lo = __int_as_float(0x7f800000); a.hi = __int_as_float(0xff800000);
+    a.bad = 0u; a.nan = 0u; a.first = 0u; a.changed = 0u;
 }
 
-// One cell: its value before the pass and after it. lo/hi are the field's declared range (range contract).
+__device__ __forceinline__ void fe_acc_bad(FeAcc& a, float after, unsigned index)
+{
+    if (fe_not_finite(after)) ++a.nan; else ++a.bad;
+    const unsigned f = ~index;
+    a.first = f > a.first ? f : a.first;
+}
+
+// Four consecutive cells (index0 .. index0 + 3): their values before the pass and after it; lo/hi the declared range.
+__device__ __forceinline__ void fe_acc_row4(FeAcc& a, const float* before, const float* after, float lo, float hi,
+    unsigned index0, bool totals_before, bool totals_after, bool range = true)
+{
+    if (totals_before) {
+        a.before += static_cast<double>((before[0] + before[1]) + (before[2] + before[3]));
+        a.before_abs += static_cast<double>((fabsf(before[0]) + fabsf(before[1])) + (fabsf(before[2]) + fabsf(before[3])));
+    }
+    if (totals_after) {
+        a.after += static_cast<double>((after[0] + after[1]) + (after[2] + after[3]));
+        a.after_abs += static_cast<double>((fabsf(after[0]) + fabsf(after[1])) + (fabsf(after[2]) + fabsf(after[3])));
+    }
+    if (range) {
+        a.lo = fminf(a.lo, fminf(fminf(after[0], after[1]), fminf(after[2], after[3])));
+        a.hi = fmaxf(a.hi, fmaxf(fmaxf(after[0], after[1]), fmaxf(after[2], after[3])));
+    }
+    const bool ok = !range || ((after[0] >= lo && after[0] <= hi) && (after[1] >= lo && after[1] <= hi) &&
+        (after[2] >= lo && after[2] <= hi) && (after[3] >= lo && after[3] <= hi));
+    if (!ok) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (!(after[q] >= lo && after[q] <= hi)) fe_acc_bad(a, after[q], index0 + q);
+        }
+    }
+    a.changed |= ((__float_as_uint(before[0]) != __float_as_uint(after[0])) | (__float_as_uint(before[1]) != __float_as_uint(after[1])) |
+                     (__float_as_uint(before[2]) != __float_as_uint(after[2])) | (__float_as_uint(before[3]) != __float_as_uint(after[3])))
+        ? 1u : 0u;
+}
+
+// One cell (the plain passes).
 __device__ __forceinline__ void fe_acc_cell(FeAcc& a, float before, float after, float lo, float hi, unsigned index,
-    bool totals_before, bool totals_after)
+    bool totals_before, bool totals_after, bool range = true)
 {
     if (totals_before) {
         a.before += static_cast<double>(before);
-        a.before_abs += fabs(static_cast<double>(before));
+        a.before_abs += static_cast<double>(fabsf(before));
     }
     if (totals_after) {
         a.after += static_cast<double>(after);
-        a.after_abs += fabs(static_cast<double>(after));
+        a.after_abs += static_cast<double>(fabsf(after));
     }
-    const bool nan = fe_not_finite(after);
-    if (!nan) {
-        const unsigned k = fe_order_key(after);
-        a.lo = k < a.lo ? k : a.lo;
-        a.hi = k > a.hi ? k : a.hi;
-    }
-    if (nan || after < lo || after > hi) {
-        if (nan) ++a.nan; else ++a.bad;
-        const unsigned f = ~index;
-        a.first = f > a.first ? f : a.first;
+    if (range) {
+        a.lo = fminf(a.lo, after);
+        a.hi = fmaxf(a.hi, after);
+        if (!(after >= lo && after <= hi)) fe_acc_bad(a, after, index);
     }
     a.changed |= (__float_as_uint(before) != __float_as_uint(after)) ? 1u : 0u;
 }
@@ -191,8 +250,9 @@ __device__ __forceinline__ void fe_acc_block(FeAcc& a, double* scratch, double* 
     const double s1 = fe_warp_sum(a.before_abs);
     const double s2 = fe_warp_sum(a.after);
     const double s3 = fe_warp_sum(a.after_abs);
-    const unsigned lo = fe_warp_min(a.lo);
-    const unsigned hi = fe_warp_max(a.hi);
+    // Float bounds to ordered keys (no finite-or-infinite value seen: the empty keys).
+    const unsigned lo = fe_warp_min(a.lo <= a.hi ? fe_order_key(a.lo) : 0xffffffffu);
+    const unsigned hi = fe_warp_max(a.lo <= a.hi ? fe_order_key(a.hi) : 0u);
     const unsigned changed = __any_sync(0xffffffffu, a.changed != 0u) ? 1u : 0u;
     const unsigned bad = __reduce_add_sync(0xffffffffu, a.bad);
     const unsigned nan = __reduce_add_sync(0xffffffffu, a.nan);
@@ -284,6 +344,354 @@ __device__ __forceinline__ void fe_acc_finish(const double* partials, int blocks
             rec->after_abs = s3;
         }
         *count = 0u;
+    }
+}
+
+// ---- the generated passes' skeletons -------------------------------------------------------------------------------
+// A pass traits struct P (generated per pass) gives the lattice (NX, NY, NZ), the tile (W warps x R rows, 128 cells
+// wide), the sources' halos (ax(k) a multiple of 4, ry(k), one RZ), the ring depth NST, the smem layout (base, pl, px),
+// which outputs carry contracts (checked(j)), and `cell(ctx, x, y, z, out, before)`, which evaluates every output of the
+// pass at one cell.
+
+// Shared-memory reads of the staged sources: ld<k>(X, Y, Z) is source k at lattice cell (X, Y, Z), which the pass's
+// halos guarantee lies in the staged box.
+template <class P>
+struct FeSlabCtx {
+    const float* sm;
+    int st[2 * P::RZ + 1];
+    int x0, y0, z;
+    float dt;
+    template <int k>
+    __device__ __forceinline__ float ld(int X, int Y, int Z) const
+    {
+        return sm[P::base(k) + st[Z - z + P::RZ] * P::pl(k) + (Y - y0 + P::ry(k)) * P::px(k) + (X - x0 + P::ax(k))];
+    }
+};
+
+// Global-memory reads (through the read-only path), for passes the TMA cannot stage (an x extent not a multiple of 4).
+template <class P>
+struct FePlainCtx {
+    const float* const* src;
+    float dt;
+    template <int k>
+    __device__ __forceinline__ float ld(int X, int Y, int Z) const
+    {
+        return __ldg(src[k] + (static_cast<fe_u64>(Z) * P::NY + static_cast<fe_u64>(Y)) * P::NX + static_cast<fe_u64>(X));
+    }
+};
+
+template <class P>
+__device__ __forceinline__ void fe_pass_contracts(FeAcc* acc, double* scratch, const FePassArgs& a)
+{
+    const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const int blocks = gridDim.x * gridDim.y * gridDim.z;
+#pragma unroll
+    for (int j = 0; j < P::NOUT; ++j) {
+        if (P::checked(j) && a.rec[j] != nullptr) {
+            fe_acc_block(acc[j], scratch, a.partials + 4 * (static_cast<fe_u64>(j) * blocks + block), a.rec[j]);
+            fe_acc_finish(a.partials + 4 * static_cast<fe_u64>(j) * blocks, blocks, a.count + j, scratch, a.rec[j],
+                (a.flags & FE_PASS_BEFORE) != 0, (a.flags & FE_PASS_AFTER) != 0);
+        }
+    }
+}
+
+// The TMA z-marching pass: a CTA owns a 128 x TY column and marches a chunk of z-planes; every source's plane (with its
+// halo) comes into a ring of NST stages by one TMA load each, NST - 2 RZ - 1 planes ahead; one mbarrier a stage counts
+// the bytes of all sources. A lane computes 4 consecutive cells on R rows and stores them as float4.
+template <class P>
+__device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
+{
+    extern __shared__ __align__(128) float fe_sm[];
+    __shared__ __align__(8) fe_u64 bar[P::NST];
+    __shared__ double scratch[4 * P::W];
+    __shared__ int failed;
+    static_assert(P::NST >= 2 * P::RZ + 2, "the ring holds 2 RZ + 1 planes and the one being fetched");
+    const int x0 = blockIdx.x * 128;
+    const int y0 = blockIdx.y * (P::W * P::R);
+    const int zb = blockIdx.z * a.zchunk;
+    const int ze = min(P::NZ, zb + a.zchunk);
+    const int zlo = max(zb - P::RZ, 0);
+    const int zhi = min(ze - 1 + P::RZ, P::NZ - 1);
+    const int nplanes = zhi - zlo + 1;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    auto issue = [&](int j) {
+        fe_mbar_expect_tx(&bar[j % P::NST], P::BYTES);
+#pragma unroll
+        for (int k = 0; k < P::NSRC; ++k) {
+            fe_tma_load_3d(fe_sm + P::base(k) + (j % P::NST) * P::pl(k), &a.map[k], &bar[j % P::NST], x0 - P::ax(k),
+                y0 - P::ry(k), zlo + j);
+        }
+    };
+    int issued = 0;
+    if (threadIdx.x == 0) {
+        failed = 0;
+        for (int s = 0; s < P::NST; ++s) fe_mbar_init(&bar[s], 1);
+        fe_fence_mbar_init();
+        issued = min(P::NST, nplanes);
+        for (int j = 0; j < issued; ++j) issue(j);
+    }
+    __syncthreads();
+    FeAcc acc[P::NOUT];
+#pragma unroll
+    for (int j = 0; j < P::NOUT; ++j) fe_acc_init(acc[j]);
+    int waited = 0;
+    auto wait_upto = [&](int j) {
+        while (waited <= j) {
+            if (!fe_mbar_wait(&bar[waited % P::NST], static_cast<unsigned>((waited / P::NST) & 1), 1u << 20)) failed = 1;
+            ++waited;
+        }
+    };
+    if (zb < ze) wait_upto(min(zb + P::RZ, P::NZ - 1) - zlo);
+    __syncthreads();
+    const int x = x0 + 4 * lane;
+    for (int z = zb; z < ze && !failed; ++z) {
+        FeSlabCtx<P> c;
+        c.sm = fe_sm;
+        c.x0 = x0;
+        c.y0 = y0;
+        c.z = z;
+        c.dt = a.dt;
+#pragma unroll
+        for (int d = -P::RZ; d <= P::RZ; ++d) c.st[d + P::RZ] = (min(max(z + d, 0), P::NZ - 1) - zlo) % P::NST;
+#pragma unroll
+        for (int r = 0; r < P::R; ++r) {
+            const int y = y0 + warp * P::R + r;
+            if (y >= P::NY || x >= P::NX) continue;
+            float o[4][P::NOUT];
+            float b[4][P::NOUT];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) P::cell(c, x + q, y, z, o[q], b[q]);
+            const fe_u64 at = static_cast<fe_u64>(x) + static_cast<fe_u64>(P::NX) * (static_cast<fe_u64>(y) + static_cast<fe_u64>(P::NY) * z);
+#pragma unroll
+            for (int j = 0; j < P::NOUT; ++j) {
+                *reinterpret_cast<float4*>(a.out[j] + at) = make_float4(o[0][j], o[1][j], o[2][j], o[3][j]);
+                if (P::checked(j) && a.rec[j] != nullptr) {
+                    const float bb[4] = {b[0][j], b[1][j], b[2][j], b[3][j]};
+                    const float oo[4] = {o[0][j], o[1][j], o[2][j], o[3][j]};
+                    fe_acc_row4(acc[j], bb, oo, a.lo[j], a.hi[j], static_cast<unsigned>(at), (a.flags & FE_PASS_BEFORE) != 0,
+                        (a.flags & FE_PASS_AFTER) != 0, (a.flags & FE_PASS_RANGE) != 0);
+                }
+            }
+        }
+        if (z + 1 < ze) wait_upto(min(z + 1 + P::RZ, P::NZ - 1) - zlo);
+        __syncthreads();
+        const int release = z - P::RZ - zlo;
+        if (threadIdx.x == 0 && !failed && release >= 0 && release + P::NST < nplanes) {
+            fe_fence_proxy_async();
+            issue(release + P::NST);
+            issued = release + P::NST + 1;
+        }
+    }
+    if (failed) {
+        if (threadIdx.x == 0) {
+            atomicOr(a.err, FE_ERR_MBAR_TIMEOUT);
+            for (int j = 0; j < issued; ++j) fe_mbar_wait(&bar[j % P::NST], static_cast<unsigned>((j / P::NST) & 1), 1u << 16);
+        }
+        return;
+    }
+    fe_pass_contracts<P>(acc, scratch, a);
+}
+
+// The plain pass: a thread a (x, y) column marching a chunk of z-planes, reads through the read-only path.
+template <class P>
+__device__ __forceinline__ void fe_plain_pass(const FePassArgs& a)
+{
+    __shared__ double scratch[4 * 8];
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    const bool live = x < P::NX && y < P::NY;
+    const int zb = blockIdx.z * a.zchunk;
+    const int ze = min(P::NZ, zb + a.zchunk);
+    FeAcc acc[P::NOUT];
+#pragma unroll
+    for (int j = 0; j < P::NOUT; ++j) fe_acc_init(acc[j]);
+    FePlainCtx<P> c;
+    c.src = a.src;
+    c.dt = a.dt;
+    for (int z = zb; live && z < ze; ++z) {
+        float o[P::NOUT];
+        float b[P::NOUT];
+        P::cell(c, x, y, z, o, b);
+        const fe_u64 at = static_cast<fe_u64>(x) + static_cast<fe_u64>(P::NX) * (static_cast<fe_u64>(y) + static_cast<fe_u64>(P::NY) * z);
+#pragma unroll
+        for (int j = 0; j < P::NOUT; ++j) {
+            a.out[j][at] = o[j];
+            if (P::checked(j) && a.rec[j] != nullptr) {
+                fe_acc_cell(acc[j], b[j], o[j], a.lo[j], a.hi[j], static_cast<unsigned>(at), (a.flags & FE_PASS_BEFORE) != 0,
+                    (a.flags & FE_PASS_AFTER) != 0, (a.flags & FE_PASS_RANGE) != 0);
+            }
+        }
+    }
+    fe_pass_contracts<P>(acc, scratch, a);
+}
+
+// A deterministic reduction of one expression over the lattice (maxof / minof / sumof): a fixed assignment of cells to
+// threads, FP64 sums, a fixed tree, then the last block folds the blocks in order. The result lands in *out.
+template <class P>
+__device__ __forceinline__ void fe_reduce_pass(const FePassArgs& a, float* out)
+{
+    __shared__ double scratch[4 * 8];
+    __shared__ unsigned last;
+    FePlainCtx<P> c;
+    c.src = a.src;
+    c.dt = a.dt;
+    const fe_u64 cells = static_cast<fe_u64>(P::NX) * P::NY * P::NZ;
+    double sum = 0.0;
+    float lo = 3.0e38f, hi = -3.0e38f;
+    const fe_u64 stride = static_cast<fe_u64>(gridDim.x) * blockDim.x;
+    for (fe_u64 i = blockIdx.x * static_cast<fe_u64>(blockDim.x) + threadIdx.x; i < cells; i += stride) {
+        const int x = static_cast<int>(i % P::NX);
+        const int y = static_cast<int>((i / P::NX) % P::NY);
+        const int z = static_cast<int>(i / (static_cast<fe_u64>(P::NX) * P::NY));
+        const float v = P::value(c, x, y, z);
+        sum += static_cast<double>(v);
+        lo = fminf(lo, v);
+        hi = fmaxf(hi, v);
+    }
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    sum = fe_warp_sum(sum);
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (lane == 0) {
+        scratch[4 * warp] = sum;
+        scratch[4 * warp + 1] = lo;
+        scratch[4 * warp + 2] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        float l = 3.0e38f, h = -3.0e38f;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+            s += scratch[4 * w];
+            l = fminf(l, static_cast<float>(scratch[4 * w + 1]));
+            h = fmaxf(h, static_cast<float>(scratch[4 * w + 2]));
+        }
+        a.partials[4 * blockIdx.x] = s;
+        a.partials[4 * blockIdx.x + 1] = l;
+        a.partials[4 * blockIdx.x + 2] = h;
+        __threadfence();
+        const unsigned done = atomicAdd(a.count, 1u);
+        last = done + 1u == gridDim.x ? 1u : 0u;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double s = 0.0;
+        float l = 3.0e38f, h = -3.0e38f;
+        for (unsigned b = 0; b < gridDim.x; ++b) {
+            const volatile double* p = a.partials + 4 * b;
+            s += p[0];
+            l = fminf(l, static_cast<float>(p[1]));
+            h = fmaxf(h, static_cast<float>(p[2]));
+        }
+        *out = P::KIND == 0 ? static_cast<float>(s) : (P::KIND == 1 ? h : l);
+        *a.count = 0u;
+    }
+}
+
+// Tridiagonal solves along x, 32 lines a block (32 consecutive y at one z): coefficient tiles come in coalesced through
+// shared memory, each thread runs Thomas' recurrence on its line (in the reference's order: the edge cell repeating, its
+// missing neighbour's coefficient landing on the diagonal), keeping c' and d' for the whole line in shared memory, so
+// global memory sees the coefficients read once and the answer written once. NXS: the x extent kept (>= NX).
+template <class P>
+__device__ __forceinline__ void fe_tridiag_x_pass(const FePassArgs& a)
+{
+    extern __shared__ __align__(128) float fe_sm[];
+    float* cs = fe_sm;                 // [NX][33]: c' of line tx at x
+    float* ds = fe_sm + P::NX * 33;    // [NX][33]: d', then the answer
+    __shared__ float ta[32][33], tb[32][33], tu[32][33], td[32][33];
+    const int tx = threadIdx.x;
+    const int y0 = blockIdx.x * 32;
+    const int z = blockIdx.y;
+    FePlainCtx<P> c;
+    c.src = a.src;
+    c.dt = a.dt;
+    float cp = 0.f, dp = 0.f;
+    for (int x0 = 0; x0 < P::NX; x0 += 32) {
+        const int x = x0 + tx;
+        for (int j = 0; j < 32; ++j) {
+            const int y = y0 + j;
+            float lo = 0.f, di = 1.f, up = 0.f, rhs = 0.f;
+            if (x < P::NX && y < P::NY) {
+                P::coef(c, x, y, z, lo, di, up, rhs);
+                if (x == 0) di += lo;
+                if (x + 1 == P::NX) di += up;
+            }
+            ta[j][tx] = lo;
+            tb[j][tx] = di;
+            tu[j][tx] = up;
+            td[j][tx] = rhs;
+        }
+        __syncthreads();
+        const int m = min(32, P::NX - x0);
+        for (int i = 0; i < m; ++i) {
+            const float lo = ta[tx][i];
+            const float den = tb[tx][i] - lo * cp;
+            dp = (td[tx][i] - lo * dp) / den;
+            cp = x0 + i + 1 == P::NX ? 0.f : tu[tx][i] / den;
+            cs[(x0 + i) * 33 + tx] = cp;
+            ds[(x0 + i) * 33 + tx] = dp;
+        }
+        __syncthreads();
+    }
+    float next = 0.f;
+    for (int i = P::NX - 1; i >= 0; --i) {
+        next = ds[i * 33 + tx] - cs[i * 33 + tx] * next;
+        ds[i * 33 + tx] = next;
+    }
+    __syncthreads();
+    for (int j = 0; j < 32; ++j) {
+        const int y = y0 + j;
+        if (y >= P::NY) break;
+        for (int x = tx; x < P::NX; x += 32) {
+            a.out[0][(static_cast<fe_u64>(z) * P::NY + y) * P::NX + x] = ds[x * 33 + j];
+        }
+    }
+}
+
+// Tridiagonal solves along y or z, a thread a line; consecutive threads take consecutive x, so every step of the
+// recurrence reads and writes whole rows (coalesced). c' goes to out[1] (scratch), d' and then the answer to out[0].
+template <class P, int AXIS>
+__device__ __forceinline__ void fe_tridiag_yz_pass(const FePassArgs& a)
+{
+    const fe_u64 k = blockIdx.x * static_cast<fe_u64>(blockDim.x) + threadIdx.x;
+    const int n = AXIS == 1 ? P::NY : P::NZ;
+    const fe_u64 lines = AXIS == 1 ? static_cast<fe_u64>(P::NX) * P::NZ : static_cast<fe_u64>(P::NX) * P::NY;
+    if (k >= lines) return;
+    const int x = static_cast<int>(k % P::NX);
+    const int other = static_cast<int>(k / P::NX); // z for y-lines, y for z-lines
+    FePlainCtx<P> c;
+    c.src = a.src;
+    c.dt = a.dt;
+    float* ans = a.out[0];
+    float* cps = a.out[1];
+    auto at = [&](int i) -> fe_u64 {
+        const int y = AXIS == 1 ? i : other;
+        const int z = AXIS == 1 ? other : i;
+        return (static_cast<fe_u64>(z) * P::NY + y) * P::NX + x;
+    };
+    float cp = 0.f, dp = 0.f;
+    for (int i = 0; i < n; ++i) {
+        const int y = AXIS == 1 ? i : other;
+        const int z = AXIS == 1 ? other : i;
+        float lo, di, up, rhs;
+        P::coef(c, x, y, z, lo, di, up, rhs);
+        if (i == 0) di += lo;
+        if (i + 1 == n) di += up;
+        const float den = di - lo * cp;
+        dp = (rhs - lo * dp) / den;
+        cp = i + 1 == n ? 0.f : up / den;
+        ans[at(i)] = dp;
+        cps[at(i)] = cp;
+    }
+    float next = 0.f;
+    for (int i = n - 1; i >= 0; --i) {
+        next = ans[at(i)] - cps[at(i)] * next;
+        ans[at(i)] = next;
     }
 }
 

@@ -127,27 +127,31 @@ __global__ void __launch_bounds__(W * 32) heat7_tma(const __grid_constant__ FeTe
             const float yr[4] = {dn.x, dn.y, dn.z, dn.w};
             const float zl[4] = {zm.x, zm.y, zm.z, zm.w};
             const float zr[4] = {zp.x, zp.y, zp.z, zp.w};
+            const bool ym = y > 0, yp = y + 1 < ny, zmv = z > 0, zpv = z + 1 < nz;
             float o[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
+                // A face past the edge adds (c - c) = +0, which leaves the sum as it is: the sum starts at +0 and a
+                // round-to-nearest sum of nonzero terms is never -0, so skipping the face and adding +0 agree to the bit.
                 const float cc = cv[q];
                 float s = 0.f;
-                if (x + q > 0) s = __fadd_rn(s, __fsub_rn(xl[q], cc));
-                if (x + q + 1 < nx) s = __fadd_rn(s, __fsub_rn(xr[q], cc));
-                if (y > 0) s = __fadd_rn(s, __fsub_rn(yl[q], cc));
-                if (y + 1 < ny) s = __fadd_rn(s, __fsub_rn(yr[q], cc));
-                if (z > 0) s = __fadd_rn(s, __fsub_rn(zl[q], cc));
-                if (z + 1 < nz) s = __fadd_rn(s, __fsub_rn(zr[q], cc));
-                const float rate = __fdiv_rn(__fmul_rn(kk, s), hh);
+                s = __fadd_rn(s, __fsub_rn(x + q > 0 ? xl[q] : cc, cc));
+                s = __fadd_rn(s, __fsub_rn(x + q + 1 < nx ? xr[q] : cc, cc));
+                s = __fadd_rn(s, __fsub_rn(ym ? yl[q] : cc, cc));
+                s = __fadd_rn(s, __fsub_rn(yp ? yr[q] : cc, cc));
+                s = __fadd_rn(s, __fsub_rn(zmv ? zl[q] : cc, cc));
+                s = __fadd_rn(s, __fsub_rn(zpv ? zr[q] : cc, cc));
+                const float ks = __fmul_rn(kk, s);
+                // (k s) / h^2: when h^2 is a power of two the host passes its exact reciprocal and the division is that
+                // multiplication, to the bit.
+                const float rate = a.inv_hh != 0.f ? __fmul_rn(ks, a.inv_hh) : __fdiv_rn(ks, hh);
                 const float d = __fmul_rn(rate, a.dt);
                 o[q] = d != 0.f ? __fadd_rn(cc, d) : cc;
-                if (check) {
-                    const unsigned idx = static_cast<unsigned>(x + q) +
-                        static_cast<unsigned>(nx) * (static_cast<unsigned>(y) + static_cast<unsigned>(ny) * static_cast<unsigned>(z));
-                    fe_acc_cell(acc, cc, o[q], a.lo, a.hi, idx, a.totals_before != 0, a.totals_after != 0);
-                }
             }
             const size_t at = static_cast<size_t>(x) + static_cast<size_t>(nx) * (static_cast<size_t>(y) + static_cast<size_t>(ny) * z);
+            if (check) {
+                fe_acc_row4(acc, cv, o, a.lo, a.hi, static_cast<unsigned>(at), a.totals_before != 0, a.totals_after != 0);
+            }
             *reinterpret_cast<float4*>(a.out + at) = make_float4(o[0], o[1], o[2], o[3]);
         }
         if (z + 1 < ze) {
@@ -217,7 +221,8 @@ __global__ void __launch_bounds__(256) heat7_plain(const float* __restrict__ T, 
         if (y + 1 < ny) s += __fsub_rn(T[i + nx], c);
         if (z > 0) s += __fsub_rn(T[i - plane], c);
         if (z + 1 < nz) s += __fsub_rn(T[i + plane], c);
-        const float rate = __fdiv_rn(__fmul_rn(kk, s), hh);
+        const float ks = __fmul_rn(kk, s);
+        const float rate = a.inv_hh != 0.f ? __fmul_rn(ks, a.inv_hh) : __fdiv_rn(ks, hh);
         const float d = __fmul_rn(rate, a.dt);
         const float o = d != 0.f ? __fadd_rn(c, d) : c;
         a.out[i] = o;
@@ -232,6 +237,20 @@ __global__ void __launch_bounds__(256) heat7_plain(const float* __restrict__ T, 
         fe_acc_block(acc, scratch, a.partials + 4 * block, a.rec);
         fe_acc_finish(a.partials, blocks, a.count, scratch, a.rec, a.totals_before != 0, a.totals_after != 0);
     }
+}
+
+// Every cell of a buffer to one value (a field's `init`).
+__global__ void __launch_bounds__(256) fill_f32(float* __restrict__ p, size_t n, float v)
+{
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        p[i] = v;
+    }
+}
+
+cudaError_t launch_fill(float* p, size_t n, float v, int sms, cudaStream_t stream)
+{
+    fill_f32<<<sms * 4, 256, 0, stream>>>(p, n, v);
+    return cudaGetLastError();
 }
 
 // ---- host side: launches (called from the C-ABI in api.cpp) ---------------------------------------------------------

@@ -14,6 +14,7 @@ struct HeatArgs {
     int nx, ny, nz;
     int zchunk;
     float k, h, dt;
+    float inv_hh;       // 1 / (h*h) when h*h is a power of two (exact), else 0: divide
     float lo, hi;       // the field's declared range (range contract)
     int totals_before;  // this pass starts the term: record the totals before it
     int totals_after;   // this pass ends the term: record the totals after it
@@ -25,6 +26,7 @@ struct HeatArgs {
 
 cudaError_t launch_heat7_tma(int variant, const FeTensorMap& map, const HeatArgs& a, cudaStream_t stream);
 cudaError_t launch_heat7_plain(const float* T, const HeatArgs& a, cudaStream_t stream);
+cudaError_t launch_fill(float* p, size_t n, float v, int sms, cudaStream_t stream);
 cudaError_t launch_copy(const float* a, float* b, size_t n, int sms, cudaStream_t stream);
 int heat7_tma_rows(int variant);
 int heat7_tma_blocks(int variant, int nx, int ny, int nz, int zchunk);

@@ -54,6 +54,32 @@ class fe_check(ctypes.Structure):
     ]
 
 
+class fe_violation(ctypes.Structure):
+    _fields_ = [
+        ("kind", _c.c_int), ("term", _c.c_int), ("field", _c.c_int), ("count", _c.c_uint32), ("first_cell", _c.c_uint32),
+        ("before", _c.c_double), ("after", _c.c_double), ("tolerance", _c.c_double), ("step", _c.c_longlong),
+        ("detail", _c.c_char * 160),
+    ]
+
+
+class fe_step_info(ctypes.Structure):
+    _fields_ = [("violations", _c.c_int), ("launches", _c.c_int), ("gpu_ms", _c.c_double)]
+
+
+class fe_field_info(ctypes.Structure):
+    _fields_ = [("init", _c.c_double), ("lo", _c.c_double), ("hi", _c.c_double), ("is_static", _c.c_int),
+                ("derived", _c.c_int), ("clamp", _c.c_int)]
+
+
+FE_RANGE, FE_NOT_FINITE, FE_CONSERVATION, FE_SUBSTEP_CAP = 0, 1, 2, 3
+FE_STEP_IGNORE_MAX_DT = 1
+
+_p = _c.c_void_p
+_s = _c.c_size_t
+_i = _c.c_int
+_d = _c.c_double
+_cs = _c.c_char_p
+
 # name -> (restype, argtypes). Every symbol include/fe.h declares is listed here (a CPU test checks both ways).
 SIGNATURES = {
     "fe_version": (_c.c_int, []),
@@ -68,6 +94,38 @@ SIGNATURES = {
     "fe_check_reset": (_c.c_int, [_c.c_void_p, _c.c_void_p]),
     "fe_check_read": (_c.c_int, [_c.c_void_p, _c.POINTER(fe_check), _c.c_void_p]),
     "fe_copy_f32": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_size_t, _c.c_void_p]),
+    "fe_law_create": (_i, [_cs, _cs, _i, _i, _i, _d, _c.POINTER(_p)]),
+    "fe_law_destroy": (None, [_p]),
+    "fe_law_ir_json": (_i, [_cs, _p, _s, _c.POINTER(_s)]),
+    "fe_law_ir_listing": (_i, [_cs, _p, _s, _c.POINTER(_s)]),
+    "fe_law_source": (_i, [_cs, _i, _i, _i, _d, _p, _s, _c.POINTER(_s)]),
+    "fe_law_compile_check": (_i, [_cs, _i, _i, _i, _d]),
+    "fe_law_field_count": (_i, [_p]),
+    "fe_law_field_id": (_i, [_p, _cs]),
+    "fe_law_field_name": (_i, [_p, _i, _p, _s]),
+    "fe_law_field_info": (_i, [_p, _i, _c.POINTER(fe_field_info)]),
+    "fe_law_term_count": (_i, [_p]),
+    "fe_law_term_name": (_i, [_p, _i, _p, _s]),
+    "fe_law_param_count": (_i, [_p]),
+    "fe_law_param_id": (_i, [_p, _cs]),
+    "fe_law_set_param": (_i, [_p, _i, _d]),
+    "fe_law_get_param": (_i, [_p, _i, _c.POINTER(_d)]),
+    "fe_law_upload": (_i, [_p, _i, _p]),
+    "fe_law_upload_device": (_i, [_p, _i, _p]),
+    "fe_law_fetch": (_i, [_p, _i, _p]),
+    "fe_law_fetch_device": (_i, [_p, _i, _p]),
+    "fe_law_field_device_ptr": (_i, [_p, _i, _c.POINTER(_p)]),
+    "fe_law_step": (_i, [_p, _d, _i, _c.POINTER(fe_step_info)]),
+    "fe_law_derive": (_i, [_p]),
+    "fe_law_check_every": (_i, [_p, _i]),
+    "fe_law_set_deferred": (_i, [_p, _i]),
+    "fe_law_sync": (_i, [_p, _c.POINTER(fe_step_info)]),
+    "fe_law_violation": (_i, [_p, _i, _c.POINTER(fe_violation)]),
+    "fe_law_substeps": (_i, [_p, _i]),
+    "fe_law_term_idle": (_i, [_p, _i]),
+    "fe_law_digest": (_i, [_p, _c.POINTER(_c.c_uint64)]),
+    "fe_law_stream": (_i, [_p, _c.POINTER(_p)]),
+    "fe_law_time_gather": (_i, [_p, _i, _i, _c.POINTER(_c.c_float)]),
 }
 
 
@@ -102,3 +160,12 @@ def check(status):
 def call(name, *args):
     """Calls fe_<name> and raises on a non-zero status."""
     return check(getattr(lib(), name)(*args))
+
+
+def text_call(name, *args):
+    """Calls a text-returning fe_* function (buf, cap, needed at the end) and returns the text."""
+    needed = ctypes.c_size_t(0)
+    check(getattr(lib(), name)(*args, None, 0, ctypes.byref(needed)))
+    buf = ctypes.create_string_buffer(needed.value)
+    check(getattr(lib(), name)(*args, buf, needed.value, ctypes.byref(needed)))
+    return buf.value.decode()

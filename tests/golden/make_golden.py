@@ -1,0 +1,154 @@
+#!/usr/bin/env python3
+"""Makes the golden fixtures: the reference's own CPU solver (its lawc, built from the reference's sources by
+`make -C oracle ref`) run on this repository's test laws (tests/laws/) from seeded starting states.
+
+    python tests/golden/make_golden.py [--lawc oracle/_ref/lawc]
+
+For each case it writes tests/golden/<case>.npz with the starting fields, the fields after the steps, and a JSON meta
+(law file, lattice, dt, steps, the substeps of the last step and the contract violations the reference reported). The
+GPU parity tests and the oracle's pin test read these; nothing here runs at test time.
+"""
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+LAWS = os.path.join(ROOT, "tests", "laws")
+sys.path.insert(0, ROOT)
+
+
+def blobs(shape, h, seed, count=4, width=0.05):
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    c = rng.uniform(0.2, 0.8, size=(count, 3))
+    a = rng.uniform(0.5, 1.0, size=count)
+    xs = [(np.arange(n) + 0.5) * h for n in (nx, ny, nz)]
+    out = np.zeros(shape)
+    for b in range(count):
+        g = [np.exp(-((xs[i] - c[b, i]) ** 2) / (2 * width * width)) for i in range(3)]
+        out += a[b] * g[2][:, None, None] * g[1][None, :, None] * g[0][None, None, :]
+    return out.astype(np.float32)
+
+
+def heston_fields(nx, ny, nz, seed, h_over=None):
+    """Per-plane option: x = ln S over ln K +- 3 (h = 6 / nx), var_j = sig_v (j + 1/2) h, put payoff, seeded model."""
+    rng = np.random.default_rng(seed)
+    h = 6.0 / nx
+    f = {k: np.zeros((nz, ny, nx), np.float32) for k in ("V", "var", "kappa", "theta", "sig_v", "rho", "r")}
+    for z in range(nz):
+        K = rng.uniform(80, 120)
+        kappa, theta, sig, rho, r = (rng.uniform(0.5, 5), rng.uniform(0.01, 0.1), rng.uniform(0.1, 1.0),
+                                     rng.uniform(-0.9, -0.1), rng.uniform(0.0, 0.05))
+        x = np.log(K) - 3 + (np.arange(nx) + 0.5) * h
+        f["V"][z] = np.maximum(K - np.exp(x), 0.0)[None, :]
+        f["var"][z] = (sig * (np.arange(ny) + 0.5) * h)[:, None]
+        f["kappa"][z], f["theta"][z], f["sig_v"][z], f["rho"][z], f["r"][z] = kappa, theta, sig, rho, r
+    return f, h
+
+
+def cases():
+    rng = np.random.default_rng(12345)
+    out = []
+    # Conduction with 3 substeps a step (dt = 2.5 max_dt).
+    n = (16, 20, 24)
+    h = 1.0 / 24
+    out.append(dict(name="heat_24", law="heat.law", shape=n, h=h, dt=2.5 * 0.4 * h * h / 6, steps=5,
+                    fields={"T": blobs(n, h, 1)}))
+    n = (9, 14, 20)
+    out.append(dict(name="ops_stencil", law="ops_stencil.law", shape=n, h=0.5, dt=0.01, steps=4,
+                    fields={"a": rng.uniform(-1, 1, n).astype(np.float32),
+                            "k": rng.uniform(0.5, 2.0, n).astype(np.float32)}))
+    out.append(dict(name="ops_point", law="ops_point.law", shape=n, h=0.5, dt=0.2, steps=4,
+                    fields={"a": rng.uniform(-1, 1, n).astype(np.float32),
+                            "b": rng.uniform(-1, 1, n).astype(np.float32)}))
+    n = (10, 12, 16)
+    f = (rng.uniform(0, 1, n) * (rng.uniform(0, 1, n) < 0.4)).astype(np.float32)
+    s = (rng.uniform(0, 1, n) < 0.2).astype(np.float32)
+    out.append(dict(name="ops_matter", law="ops_matter.law", shape=n, h=0.5, dt=0.01, steps=4, fields={"f": f, "s": s}))
+    n = (4, 32, 32)
+    out.append(dict(name="fhn_32", law="fhn_rk4.law", shape=n, h=2.0 / 32, dt=0.05, steps=3,
+                    fields={"u": rng.normal(size=n).astype(np.float32), "v": rng.normal(size=n).astype(np.float32)}))
+    n = (3, 4, 64)
+    x = (np.arange(64) + 0.5) / 64
+    T = (1 + np.cos(4 * np.pi * x))[None, None, :] + 0.01 * rng.normal(size=n)
+    out.append(dict(name="cn_64", law="crank_nicolson.law", shape=n, h=1.0 / 64, dt=0.01, steps=5,
+                    fields={"T": T.astype(np.float32)}))
+    n = (20, 24, 8)
+    out.append(dict(name="implicit_yz", law="implicit_yz.law", shape=n, h=1.0 / 24, dt=0.001, steps=3,
+                    fields={"T": blobs(n, 1.0 / 24, 2, width=0.15)}))
+    f, h = heston_fields(32, 16, 3, 7)
+    out.append(dict(name="heston_douglas", law="heston_douglas.law", shape=(3, 16, 32), h=h, dt=0.01, steps=4, fields=f))
+    out.append(dict(name="heston_hv", law="heston_hv.law", shape=(3, 16, 32), h=h, dt=0.01, steps=4, fields=f))
+    return out
+
+
+def run(case, lawc, work):
+    law = os.path.join(LAWS, case["law"])
+    nz, ny, nx = case["shape"]
+    scene = os.path.join(work, "scene")
+    with open(scene, "w") as fh:
+        fh.write(f"grid {nx} {ny} {nz} {case['h']!r}\nlaw {law}\n")
+    init = os.path.join(work, "init")
+    os.makedirs(init, exist_ok=True)
+    for name, arr in case["fields"].items():
+        np.ascontiguousarray(arr, dtype=np.float32).tofile(os.path.join(init, name + ".bin"))
+    dump = os.path.join(work, "dump")
+    js = os.path.join(work, "t.json")
+    cmd = [lawc, "--scene", scene, "--init", init, "--steps", str(case["steps"]), "--dt", repr(case["dt"]), "--dump", dump,
+           "--json", js]
+    res = subprocess.run(cmd, capture_output=True, text=True, env=dict(os.environ, OMP_NUM_THREADS="4"))
+    if res.returncode != 0:
+        raise RuntimeError(f"{case['name']}: lawc failed\n{res.stdout}\n{res.stderr}")
+    meta_dump = json.load(open(os.path.join(dump, f"step_{case['steps']}", "meta.json")))
+    final = {f: np.fromfile(os.path.join(dump, f"step_{case['steps']}", f + ".bin"), dtype=np.float32).reshape(case["shape"])
+             for f in meta_dump["fields"]}
+    timing = json.load(open(js))
+    meta = dict(name=case["name"], law=case["law"], shape=list(case["shape"]), h=case["h"], dt=case["dt"], steps=case["steps"],
+                substeps=timing["substeps"], violations=timing["violations"], fields=meta_dump["fields"],
+                made_by="the reference's lawc (its OpenMP CPU Solver), OMP_NUM_THREADS=4")
+    arrays = {f"init_{k}": np.asarray(v, np.float32) for k, v in case["fields"].items()}
+    arrays.update({f"final_{k}": v for k, v in final.items()})
+    np.savez_compressed(os.path.join(HERE, case["name"] + ".npz"), meta=json.dumps(meta), **arrays)
+    return meta
+
+
+def ir_fixtures(lawc):
+    """The reference's IR JSON (lawc --ir-json) of every test law: the lowering's golden vectors."""
+    out_dir = os.path.join(HERE, "ir")
+    os.makedirs(out_dir, exist_ok=True)
+    for name in sorted(os.listdir(LAWS)):
+        if not name.endswith(".law"):
+            continue
+        out = os.path.join(out_dir, name[:-4] + ".json")
+        subprocess.run([lawc, "--ir-json", out, os.path.join(LAWS, name)], check=True, capture_output=True)
+        print("ir", name)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--lawc", default=os.path.join(ROOT, "oracle", "_ref", "lawc"))
+    ap.add_argument("--only", default="")
+    args = ap.parse_args()
+    if not os.path.exists(args.lawc):
+        sys.exit(f"no reference solver at {args.lawc}: build it with `make -C oracle ref`")
+    ir_fixtures(args.lawc)
+    for case in cases():
+        if args.only and case["name"] not in args.only.split(","):
+            continue
+        work = tempfile.mkdtemp(prefix="fe_golden_")
+        try:
+            meta = run(case, args.lawc, work)
+            print(case["name"], "substeps", meta["substeps"], "violations", meta["violations"])
+        finally:
+            shutil.rmtree(work, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,168 @@
+"""The law backend on the GPU against the reference's own CPU solver (golden fixtures made by its lawc), the hand-written
+kernel, itself (determinism) and the contracts it must catch."""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
+# Relative tolerance against the reference's CPU solver (which computes every op in double and stores float): the
+# reference's own gate holds one op to 2e-5 and a whole law to 1e-4 (src/tests/cuda_parity_smoke.cpp:114-117, 159-160).
+TOLERANCE = {"heat_24": 1e-6, "ops_stencil": 2e-5, "ops_matter": 2e-5, "cn_64": 2e-5, "implicit_yz": 2e-5}
+
+
+def load(path):
+    z = np.load(path)
+    meta = json.loads(str(z["meta"]))
+    init = {k[5:]: z[k] for k in z.files if k.startswith("init_")}
+    final = {k[6:]: z[k] for k in z.files if k.startswith("final_")}
+    return meta, init, final
+
+
+def run_case(meta, init, steps=None):
+    from fieldcuda.solver import Solver
+    nz, ny, nx = meta["shape"]
+    s = Solver(open(os.path.join(ROOT, "tests", "laws", meta["law"])).read(), nx, ny, nz, meta["h"], meta["law"])
+    for name, arr in init.items():
+        s.set_field(name, arr)
+    for _ in range(steps or meta["steps"]):
+        s.step(meta["dt"])
+    return s
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p)[:-4])
+def test_matches_reference_cpu_solver(cuda, path):
+    meta, init, final = load(path)
+    s = run_case(meta, init)
+    tol = TOLERANCE.get(meta["name"], 1e-4)
+    for name, want in final.items():
+        got = s.values(name)
+        scale = max(float(np.abs(want).max()), 1e-6)
+        rel = float(np.abs(got.astype(np.float64) - want).max()) / scale
+        assert rel <= tol, f"{meta['name']}:{name} relative difference {rel:.3g} > {tol}"
+    assert s.last_substeps() == meta["substeps"], (s.last_substeps(), meta["substeps"])
+    assert len(s.violations()) == 0 and meta["violations"] == 0, s.violations()
+    s.close()
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p)[:-4])
+def test_two_runs_are_bit_identical(cuda, path):
+    meta, init, _ = load(path)
+    a = run_case(meta, init)
+    b = run_case(meta, init)
+    assert a.digest() == b.digest()
+    a.close()
+    b.close()
+
+
+def test_engine_heat_bit_identical_to_handwritten_kernel(cuda):
+    """The generated step of `d T = diffuse(D, T)` and the hand-written kernel do the same arithmetic in the same order:
+    equal to the bit (the reference's own check: bench/stencil_bench.cpp:291-294)."""
+    import torch
+    from fieldcuda import kernels
+    from fieldcuda.solver import Solver
+    from oracle import heat as oh
+    for n in (64, 96):
+        h = 1.0 / n
+        dt = 0.4 * h * h / 6.0
+        T0 = oh.gaussian_blobs(n, h, seed=3)
+        s = Solver(open(os.path.join(ROOT, "tests", "laws", "heat.law")).read(), n, n, n, h)
+        s.set_field("T", T0)
+        a = torch.from_numpy(T0).cuda()
+        b = torch.empty_like(a)
+        ws = kernels.heat7_workspace(T0.shape, 0, 16)
+        for _ in range(7):
+            s.step(dt)
+            kernels.heat7_step(a, b, 1.0, h, dt, variant=0, zchunk=16, check=0, workspace=ws)
+            a, b = b, a
+        torch.cuda.synchronize()
+        got = s.values("T")
+        assert np.array_equal(got.view(np.uint32), a.cpu().numpy().view(np.uint32))
+        s.close()
+
+
+def test_conservation_violation_is_reported(cuda):
+    from fieldcuda.solver import Solver
+    law = ("field T init 1 range -1e6 1e6\nparam leak = 0.5\nterm leaky\n  d T = diffuse(1, T) - leak * T\n  conserves T\n")
+    s = Solver(law, 16, 12, 8, 0.1)
+    s.set_field("T", np.random.default_rng(0).uniform(1, 2, (8, 12, 16)).astype(np.float32))
+    s.step(0.001)
+    v = s.violations()
+    assert any(x.kind == "conservation" and x.term == "leaky" and x.field == "T" for x in v), v
+    s.set_param("leak", 0.0)
+    s.step(0.001)
+    assert not s.violations()
+    s.close()
+
+
+def test_range_and_nan_violations_are_reported(cuda):
+    from fieldcuda.solver import Solver
+    law = "field a init 0 range 0 1\nterm grow\n  d a = 2 * a + 1\n"
+    s = Solver(law, 8, 8, 4, 1.0)
+    s.step(0.25)  # 0 -> 0.25: in range
+    assert not s.violations()
+    s.step(1.0)   # 0.25 -> 1.75: out of range everywhere
+    v = s.violations()
+    assert len(v) == 1 and v[0].kind == "range" and v[0].count == 8 * 8 * 4 and v[0].first_cell == 0
+    bad = np.zeros((4, 8, 8), np.float32)
+    bad[1, 2, 3] = np.nan
+    s.set_field("a", bad)
+    s.step(0.0)
+    v = s.violations()
+    assert len(v) == 1 and v[0].kind == "not-finite" and v[0].first_cell == 3 + 8 * (2 + 8 * 1)
+    s.close()
+
+
+def test_substep_cap_and_ignoring_max_dt(cuda):
+    from fieldcuda.solver import Solver
+    law = "field T init 0 range -1e9 1e9\nterm c\n  d T = diffuse(1, T)\n  max_dt = 0.1 * h * h\n"
+    s = Solver(law, 8, 8, 8, 0.01)
+    s.set_field("T", np.random.default_rng(1).uniform(0, 1, (8, 8, 8)).astype(np.float32))
+    s.step(1e-6)
+    assert s.last_substeps() == [1]
+    s.step(1e-4)  # max_dt = 1e-5: 10 substeps
+    assert s.last_substeps() == [10]
+    s.step(1.0)   # 100000 substeps wanted: capped
+    assert s.last_substeps() == [4096]
+    assert any(v.kind == "substep-cap" for v in s.violations())
+    s.set_respect_max_dt(False)
+    s.step(1e-4)
+    assert s.last_substeps() == [1]
+    s.close()
+
+
+def test_idle_term_is_not_dispatched(cuda):
+    """A term whose every equation is zero given the fields' bounds does nothing (LawBounds.cpp; CudaSolver.cpp:590)."""
+    from fieldcuda.solver import Solver
+    law = "field T init 5 range -1e9 1e9\nfield m init 0 range -1e9 1e9\nterm heat\n  d T = diffuse(1, T)\nterm mana\n  d T = 3 * m\n"
+    s = Solver(law, 8, 8, 8, 1.0)
+    s.step(0.1)
+    assert s.idle_terms() == [True, True]  # T uniform: no flux; m all zero
+    T = np.full((8, 8, 8), 5, np.float32)
+    T[4, 4, 4] = 6
+    s.set_field("T", T)
+    s.step(0.01)
+    assert s.idle_terms() == [False, True]
+    s.close()
+
+
+def test_deferred_judging_keeps_steps_off_the_host(cuda):
+    from fieldcuda.solver import Solver
+    law = "field T init 1 range -1e6 1e6\nparam leak = 0\nterm t\n  d T = diffuse(1, T) - leak * T\n  conserves T\n"
+    s = Solver(law, 16, 8, 8, 0.1)
+    s.set_field("T", np.random.default_rng(2).uniform(1, 2, (8, 8, 16)).astype(np.float32))
+    s.set_deferred(True)
+    for i in range(5):
+        if i == 3:
+            s.set_param("leak", 1.0)
+        s.step(0.001)
+    s.sync()
+    v = s.violations()
+    assert [x.step for x in v if x.kind == "conservation"] == [3, 4], v
+    s.close()
