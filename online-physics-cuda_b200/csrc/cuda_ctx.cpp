@@ -108,6 +108,10 @@ bool device_ready(std::string& why)
             std::to_string(minor);
         return false;
     }
+    // The driver-API calls (modules, launches) run in the runtime's primary context: make it current on this thread.
+    if (!cuda_ok(cudaSetDevice(dev), "cudaSetDevice", why) || !cuda_ok(cudaFree(nullptr), "context", why)) {
+        return false;
+    }
     return true;
 }
 

@@ -1,0 +1,453 @@
+"""A CPU restatement of the reference's law solver, over the reference's IR JSON. Test infrastructure only.
+
+It evaluates a law the way the reference's CPU solver does — every whole-lattice op in double, stored as float32
+between ops (src/field/Law.cpp:757-1468), all-zero results turned into the scalar 0 (`settle`, Law.cpp:554-563), the
+cheaper factor of a product first (Law.cpp:818-830) — and steps it as its Solver does: terms in order (Lie splitting),
+substeps from max_dt capped at 4096, gather-then-apply with `delta = float(value * sub_dt)`, `T += delta` in float,
+the conserved totals in double and the range contract after each term (src/field/Solver.cpp:273-461).
+
+Input: the IR JSON the reference's lawc writes (and libfe_b200's fe_law_ir_json writes identically). Fields are numpy
+arrays shaped (nz, ny, nx). Pinned bit for bit against the reference's own solver in tests/test_oracle_pin.py.
+"""
+import json
+import math
+
+import numpy as np
+
+F32 = np.float32
+
+
+class Law:
+    def __init__(self, ir_json):
+        ir = json.loads(ir_json) if isinstance(ir_json, str) else ir_json
+        self.ir = ir
+        self.insts = ir["insts"]
+        self.fields = [f["name"] for f in ir["fields"]]
+        self.decls = ir["fields"]
+        self.params = [p["value"] for p in ir["params"]]
+        self.param_names = [p["name"] for p in ir["params"]]
+        self.terms = ir["terms"]
+        self.derives = ir["derives"]
+        self._cost = [None] * len(self.insts)
+
+    def cost(self, i):
+        """Subtree size, everything inlined (the reference's node cost, Law.cpp:1518-1521)."""
+        if self._cost[i] is None:
+            self._cost[i] = 1 + sum(self.cost(a) for a in self.insts[i]["args"])
+        return self._cost[i]
+
+
+def _settle(a):
+    a = np.asarray(a, dtype=F32)
+    return 0.0 if not np.any(a != 0) else a
+
+
+def _is_scalar(v):
+    return not isinstance(v, np.ndarray)
+
+
+def _uniform(v):
+    return _is_scalar(v) or bool(np.all(v == v.reshape(-1)[0]))
+
+
+class Evaluator:
+    """One gather: every value of the pre-state computed once (the reference's epoch sharing)."""
+
+    def __init__(self, law, fields, zero, h, dt):
+        self.law = law
+        self.fields = fields
+        self.zero = zero
+        self.h = h
+        self.dt = dt
+        self.memo = {}
+        self.shape = next(iter(fields.values())).shape if fields else (1, 1, 1)
+
+    def __call__(self, i):
+        if i not in self.memo:
+            self.memo[i] = self._eval(i)
+        return self.memo[i]
+
+    def _arr(self, v):
+        return np.full(self.shape, v, dtype=np.float64) if _is_scalar(v) else v.astype(np.float64)
+
+    def _eval(self, i):
+        ins = self.law.insts[i]
+        op = ins["op"]
+        a = ins["args"]
+        h = self.h
+        nz, ny, nx = self.shape
+        if op == "const":
+            return float(ins["number"])
+        if op == "param":
+            return float(self.law.params[ins["index"]])
+        if op == "h":
+            return float(h)
+        if op == "dt":
+            return float(self.dt)
+        if op == "field":
+            f = self.law.fields[ins["index"]]
+            return 0.0 if self.zero[f] else self.fields[f]
+        if op == "rim":
+            z, y, x = np.indices(self.shape)
+            r = ((x == 0) | (y == 0) | (z == 0) | (x == nx - 1) | (y == ny - 1) | (z == nz - 1)).astype(F32)
+            return _settle(r)
+        unary = {
+            "neg": lambda v: -v, "abs": np.abs, "sqrt": lambda v: np.sqrt(np.maximum(0.0, v)),
+            "exp": lambda v: np.exp(np.minimum(v, 80.0)), "log": lambda v: np.log(np.maximum(v, 1e-30)),
+            "step": lambda v: np.where(v > 0.0, 1.0, 0.0), "pos": lambda v: np.maximum(v, 0.0),
+        }
+        if op in unary:
+            v = self(a[0])
+            if _is_scalar(v):
+                return float(unary[op](np.float64(v)))
+            with np.errstate(all="ignore"):
+                return _settle(unary[op](v.astype(np.float64)).astype(F32))
+        if op == "mul":
+            # The cheaper factor first; a scalar zero ends it without looking at the other (Law.cpp:818-830).
+            swap = self.law.cost(a[1]) < self.law.cost(a[0])
+            first, second = (a[1], a[0]) if swap else (a[0], a[1])
+            fa = self(first)
+            if _is_scalar(fa) and fa == 0.0:
+                return 0.0
+            fb = self(second)
+            if _is_scalar(fb) and fb == 0.0:
+                return 0.0
+            x, y = (fb, fa) if swap else (fa, fb)
+            if _is_scalar(x) and _is_scalar(y):
+                return x * y
+            with np.errstate(all="ignore"):
+                return _settle((np.float64(x) if _is_scalar(x) else x.astype(np.float64)) *
+                               (np.float64(y) if _is_scalar(y) else y.astype(np.float64)))
+        binary = {
+            "add": lambda p, q: p + q, "sub": lambda p, q: p - q,
+            "div": lambda p, q: np.where(q == 0.0, 0.0, p / np.where(q == 0.0, 1.0, q)),
+            "pow": lambda p, q: np.power(p, q), "min": np.minimum, "max": np.maximum,
+        }
+        if op in binary:
+            x, y = self(a[0]), self(a[1])
+            with np.errstate(all="ignore"):
+                if _is_scalar(x) and _is_scalar(y):
+                    return float(binary[op](np.float64(x), np.float64(y)))
+                xx = np.float64(x) if _is_scalar(x) else x.astype(np.float64)
+                yy = np.float64(y) if _is_scalar(y) else y.astype(np.float64)
+                return _settle(np.asarray(binary[op](xx, yy)).astype(F32))
+        if op == "clamp":
+            x, lo, hi = self(a[0]), self(a[1]), self(a[2])
+            if all(_is_scalar(v) for v in (x, lo, hi)):
+                return float(min(max(x, lo), max(lo, hi)))
+            xx, ll, hh = self._arr(x), self._arr(lo), self._arr(hi)
+            return _settle(np.minimum(np.maximum(xx, ll), np.maximum(ll, hh)).astype(F32))
+        if op == "shift":
+            v = self(a[0])
+            if _is_scalar(v):
+                return v
+            dx, dy, dz = ins["offset"]
+            zi = np.clip(np.arange(nz) + dz, 0, nz - 1)
+            yi = np.clip(np.arange(ny) + dy, 0, ny - 1)
+            xi = np.clip(np.arange(nx) + dx, 0, nx - 1)
+            return _settle(v[zi][:, yi][:, :, xi])
+        if op in ("lap", "gx", "gy", "gz"):
+            v = self(a[0])
+            if _uniform(v):
+                return 0.0
+            return _settle(self._stencil(op, v))
+        if op == "diffuse":
+            return self._diffuse(self(a[0]), self(a[1]))
+        if op == "adv":
+            return self._adv(self(a[0]), self(a[1]), self(a[2]), self(a[3]))
+        if op == "tridiag":
+            return self._tridiag(ins["index"], *(self(x) for x in a))
+        if op in ("maxof", "minof", "sumof"):
+            v = self(a[0])
+            if _is_scalar(v):
+                return v * (nx * ny * nz) if op == "sumof" else v
+            flat = v.reshape(-1).astype(np.float64)
+            if op == "sumof":
+                acc = 0.0
+                for x in flat:  # in order, in double (Law.cpp:1449-1466)
+                    acc += x
+                return acc
+            return float(flat.max() if op == "maxof" else flat.min())
+        if op in ("fall", "spread", "topple"):
+            return getattr(self, "_" + op)(*(self(x) for x in a))
+        raise NotImplementedError(f"the oracle does not restate '{op}'")
+
+    # ---- stencils (Law.cpp:947-985) ----------------------------------------------------------------------------------
+    def _neighbours(self, v):
+        nz, ny, nx = self.shape
+        x = np.arange(nx)
+        y = np.arange(ny)
+        z = np.arange(nz)
+        xm, xp = np.maximum(x - 1, 0), np.minimum(x + 1, nx - 1)
+        ym, yp = np.maximum(y - 1, 0), np.minimum(y + 1, ny - 1)
+        zm, zp = np.maximum(z - 1, 0), np.minimum(z + 1, nz - 1)
+        return (v[:, :, xm], v[:, :, xp], v[:, ym, :], v[:, yp, :], v[zm], v[zp], (xm, xp, ym, yp, zm, zp))
+
+    def _stencil(self, op, v):
+        h = self.h
+        d = v.astype(np.float64)
+        vxm, vxp, vym, vyp, vzm, vzp, (xm, xp, ym, yp, zm, zp) = self._neighbours(d)
+        nz, ny, nx = self.shape
+        with np.errstate(all="ignore"):
+            if op == "lap":
+                out = (vxm + vxp + vym + vyp + vzm + vzp - 6.0 * d) / (h * h)
+            elif op == "gx":
+                out = (vxp - vxm) / (h * (xp - xm).astype(np.float64))[None, None, :]
+            elif op == "gy":
+                out = (vyp - vym) / (h * (yp - ym).astype(np.float64))[None, :, None] if ny > 1 else np.zeros(self.shape)
+            else:
+                out = (vzp - vzm) / (h * (zp - zm).astype(np.float64))[:, None, None] if nz > 1 else np.zeros(self.shape)
+        return np.where(np.isfinite(out), out, 0.0).astype(F32)
+
+    def _active_planes(self, v):
+        nz = self.shape[0]
+        flat = np.array([bool(np.all(v[z] == v[z].reshape(-1)[0])) for z in range(nz)])
+        level = np.array([v[z].reshape(-1)[0] for z in range(nz)])
+        act = np.zeros(nz, bool)
+        for z in range(nz):
+            m = not flat[z]
+            if z > 0:
+                m = m or not flat[z - 1] or level[z - 1] != level[z]
+            if z + 1 < nz:
+                m = m or not flat[z + 1] or level[z + 1] != level[z]
+            act[z] = m
+        return act
+
+    def _diffuse(self, k, f):
+        """Flux form with the harmonic face conductivity, in double (Law.cpp:986-1018)."""
+        if _uniform(f):
+            return 0.0
+        h = self.h
+        nz, ny, nx = self.shape
+        v = f.astype(np.float64)
+        kk = self._arr(k)
+        acc = np.zeros(self.shape)
+        for axis, n in ((2, nx), (1, ny), (0, nz)):
+            for sign in (-1, 1):
+                nb = np.roll(v, -sign, axis=axis)
+                kb = np.roll(kk, -sign, axis=axis)
+                with np.errstate(all="ignore"):
+                    kf = np.where(kk + kb > 0.0, 2.0 * kk * kb / np.where(kk + kb > 0.0, kk + kb, 1.0), 0.0)
+                idx = np.arange(n) + sign
+                valid = ((idx >= 0) & (idx < n))
+                shape = [1, 1, 1]
+                shape[axis] = n
+                acc += np.where(valid.reshape(shape), kf * (nb - v), 0.0)
+        out = (acc / (h * h)).astype(F32)
+        act = self._active_planes(f)
+        out[~act] = 0.0
+        return _settle(out)
+
+    def _adv(self, f, u, w, s):
+        """Upwind -(u . grad F) (Law.cpp:1019-1040)."""
+        if _uniform(f):
+            return 0.0
+        h = self.h
+        v = f.astype(np.float64)
+        out = np.zeros(self.shape)
+        for axis, speed in ((2, u), (1, w), (0, s)):
+            sp = self._arr(speed)
+            n = self.shape[axis]
+            c = np.indices(self.shape)[axis]
+            lo = np.roll(v, 1, axis=axis)
+            hi = np.roll(v, -1, axis=axis)
+            up = np.where(sp > 0.0, np.where(c > 0, sp * (v - lo) / h, 0.0), np.where(c + 1 < n, sp * (hi - v) / h, 0.0))
+            out += up
+        return _settle((-out).astype(F32))
+
+    def _tridiag(self, axis, lo, di, up, rhs):
+        """Thomas' algorithm in double, a line at a time, the edge cell repeating (Law.cpp:1098-1138)."""
+        L, D, U, R = (np.moveaxis(self._arr(x), 2 - axis, -1) for x in (lo, di, up, rhs))
+        n = L.shape[-1]
+        c = np.zeros(L.shape)
+        d = np.zeros(L.shape)
+        for i in range(n):
+            a = L[..., i]
+            b = D[..., i] + (a if i == 0 else 0.0) + (U[..., i] if i + 1 == n else 0.0)
+            m = b if i == 0 else b - a * c[..., i - 1]
+            c[..., i] = 0.0 if i + 1 == n else U[..., i] / m
+            d[..., i] = (R[..., i] - (0.0 if i == 0 else a * d[..., i - 1])) / m
+        x = np.zeros(L.shape, dtype=F32)
+        nxt = np.zeros(L.shape[:-1])
+        for i in range(n - 1, -1, -1):
+            nxt = d[..., i] - c[..., i] * nxt
+            x[..., i] = nxt.astype(F32)
+        return np.moveaxis(x, -1, 2 - axis)
+
+    # ---- matter ops (Law.cpp:1192-1334) -----------------------------------------------------------------------------
+    def _fall(self, f, b, speed):
+        nz = self.shape[0]
+        if _is_scalar(f) or nz < 2:
+            return 0.0
+        h = self.h
+        fv = f.astype(np.float64)
+        bb = self._arr(b)
+        sp = self._arr(speed)
+        wide = np.zeros(self.shape)
+        free = np.clip(1.0 - bb[:-1] - fv[:-1], 0.0, 1.0)
+        wide[1:] = np.maximum(0.0, sp[1:]) / h * np.maximum(0.0, fv[1:]) * free
+        out = (0.0 - wide).astype(F32)
+        out[:-1] = (out[:-1] + wide[1:]).astype(F32)
+        return _settle(out)
+
+    def _spread(self, f, b, k):
+        if _uniform(f):
+            return 0.0
+        h = self.h
+        fv = f.astype(np.float64)
+        bb = self._arr(b)
+        kk = self._arr(k)
+        nz, ny, nx = self.shape
+
+        def flux(fa, fc, ba, bc, ka, kc, fra, frc):
+            r_is_c = fa > fc
+            free = np.clip(1.0 - np.where(r_is_c, bc, ba) - np.where(r_is_c, frc, fra), 0.0, 1.0)
+            kf = 0.5 * (np.maximum(0.0, ka) + np.maximum(0.0, kc))
+            return kf / (h * h) * (fa - fc) * free
+
+        wx = np.zeros(self.shape)
+        wy = np.zeros(self.shape)
+        wx[:, :, :-1] = flux(fv[:, :, :-1], fv[:, :, 1:], bb[:, :, :-1], bb[:, :, 1:], kk[:, :, :-1], kk[:, :, 1:], fv[:, :, :-1], fv[:, :, 1:])
+        wy[:, :-1, :] = flux(fv[:, :-1, :], fv[:, 1:, :], bb[:, :-1, :], bb[:, 1:, :], kk[:, :-1, :], kk[:, 1:, :], fv[:, :-1, :], fv[:, 1:, :])
+        out = np.zeros(self.shape, F32)
+        out[:, 1:, :] = (out[:, 1:, :] + wy[:, :-1, :]).astype(F32)
+        out[:, :, 1:] = (out[:, :, 1:] + wx[:, :, :-1]).astype(F32)
+        out = (out - wx).astype(F32)
+        out = (out - wy).astype(F32)
+        return _settle(out)
+
+    def _topple(self, f, b, rate):
+        nz, ny, nx = self.shape
+        if _is_scalar(f) or nz < 2:
+            return 0.0
+        h = self.h
+        fv = f.astype(np.float64)
+        bb = self._arr(b)
+        rr = self._arr(rate)
+        room = np.clip(1.0 - bb - fv, 0.0, 1.0)
+        wide = np.zeros((4,) + self.shape)
+        z, y, x = np.indices(self.shape)
+        below_room = np.zeros(self.shape)
+        below_room[1:] = room[:-1]
+        can = (fv > 0.0) & (z > 0) & ~(below_room > 0.01)
+        shifts = [(-1, 0), (1, 0), (0, -1), (0, 1)]
+        for s, (sx, sy) in enumerate(shifts):
+            jx = x + sx
+            jy = y + sy
+            inside = (jx >= 0) & (jx < nx) & (jy >= 0) & (jy < ny)
+            jxc = np.clip(jx, 0, nx - 1)
+            jyc = np.clip(jy, 0, ny - 1)
+            zc = np.maximum(z - 1, 0)
+            rj = room[z, jyc, jxc]
+            rjb = room[zc, jyc, jxc]
+            w = 0.25 * np.maximum(0.0, rr) / h * fv * np.minimum(rj, rjb)
+            wide[s] = np.where(can & inside, w, 0.0)
+        out = np.zeros(self.shape)
+        for s in range(4):
+            out -= wide[s]
+        up = np.zeros((4,) + self.shape)
+        up[:, :-1] = wide[:, 1:]
+        add = np.zeros(self.shape)
+        # cell (x, y, z) gains what slid off (x+1, y, z+1) going -x, (x-1, y, z+1) going +x, (x, y+1, z+1) going -y,
+        # (x, y-1, z+1) going +y, in that order.
+        t = np.zeros(self.shape)
+        t[:, :, :-1] = up[0][:, :, 1:]
+        add = add + t
+        t = np.zeros(self.shape)
+        t[:, :, 1:] = up[1][:, :, :-1]
+        add = add + t
+        t = np.zeros(self.shape)
+        t[:, :-1, :] = up[2][:, 1:, :]
+        add = add + t
+        t = np.zeros(self.shape)
+        t[:, 1:, :] = up[3][:, :-1, :]
+        add = add + t
+        out = out + add
+        return _settle(out.astype(F32))
+
+
+class Solver:
+    """Steps a law like the reference's CPU Solver (src/field/Solver.cpp:273-461)."""
+
+    MAX_SUBSTEPS = 4096
+
+    def __init__(self, law, shape, h):
+        self.law = law
+        self.h = h
+        self.shape = shape
+        self.fields = {}
+        for d in law.decls:
+            self.fields[d["name"]] = np.full(shape, F32(d["init"]), dtype=F32)
+        self.violations = []
+        self.substeps = [1] * len(law.terms)
+
+    def _zero(self):
+        return {k: not np.any(v != 0) for k, v in self.fields.items()}
+
+    def step(self, dt):
+        self.violations = []
+        for t, term in enumerate(self.law.terms):
+            self._integrate(t, term, dt)
+        for d in self.law.derives:
+            ev = Evaluator(self.law, self.fields, self._zero(), self.h, 0.0)
+            target = self.law.fields[d["equations"][0][0]]
+            v = ev(d["equations"][0][1])
+            old = self.fields[target].astype(np.float64) if d["accumulate"] else 0.0
+            self.fields[target] = (old + (np.float64(v) if _is_scalar(v) else v.astype(np.float64))).astype(F32) * np.ones(self.shape, F32)
+
+    def _integrate(self, t, term, dt):
+        law = self.law
+        self.substeps[t] = 1
+        count = 1
+        if term["max_dt"] >= 0:
+            ev = Evaluator(law, self.fields, self._zero(), self.h, 0.0)
+            limit = ev(term["max_dt"])
+            if _is_scalar(limit) and limit > 0.0 and math.isfinite(limit) and dt > limit:
+                wanted = math.ceil(dt / limit)
+                if wanted > self.MAX_SUBSTEPS:
+                    self.violations.append(("substep-cap", t))
+                    count = self.MAX_SUBSTEPS
+                else:
+                    count = int(wanted)
+        self.substeps[t] = count
+        sub_dt = dt / count
+        before = None
+        touched = False
+        for _ in range(count):
+            ev = Evaluator(law, self.fields, self._zero(), self.h, sub_dt)
+            deltas = []
+            for target, value in term["equations"]:
+                v = ev(value)
+                if _is_scalar(v) and v == 0.0:
+                    deltas.append(None)
+                    continue
+                if _is_scalar(v):
+                    deltas.append(np.full(self.shape, F32(v * sub_dt), dtype=F32))
+                else:
+                    deltas.append((v.astype(np.float64) * sub_dt).astype(F32))
+            if all(d is None for d in deltas):
+                break
+            if not touched:
+                before = [(sum(float(np.sum(self.fields[law.fields[f]], dtype=np.float64)) for f in g),
+                           sum(float(np.sum(np.abs(self.fields[law.fields[f]].astype(np.float64)))) for f in g))
+                          for g in term["conserves"]]
+            touched = True
+            for (target, _), d in zip(term["equations"], deltas):
+                if d is not None:
+                    name = law.fields[target]
+                    self.fields[name] = (self.fields[name] + d).astype(F32)
+        if before is not None:
+            for g, (b, scale) in zip(term["conserves"], before):
+                after = sum(float(np.sum(self.fields[law.fields[f]], dtype=np.float64)) for f in g)
+                tol = 1e-5 * (scale + 1.0) * math.sqrt(count)
+                if abs(after - b) > tol:
+                    self.violations.append(("conservation", t))
+        if touched:
+            for w in term["writes"]:
+                d = law.decls[w]
+                v = self.fields[d["name"]]
+                bad = ~np.isfinite(v) | (v < d["lo"]) | (v > d["hi"])
+                if d["clamp"]:
+                    self.fields[d["name"]] = np.clip(v, d["lo"], d["hi"]).astype(F32)
+                elif np.any(bad):
+                    self.violations.append(("not-finite" if np.any(~np.isfinite(v)) else "range", t))

@@ -1,0 +1,49 @@
+"""Pins the oracle: its restatement of the reference's CPU solver against the reference's own outputs (golden fixtures
+made by the reference's lawc), bit for bit, and the heat restatement against it."""
+import glob
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
+
+
+def load(path):
+    z = np.load(path)
+    meta = json.loads(str(z["meta"]))
+    return meta, {k[5:]: z[k] for k in z.files if k.startswith("init_")}, {k[6:]: z[k] for k in z.files if k.startswith("final_")}
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p)[:-4])
+def test_oracle_reproduces_reference_solver(path):
+    from oracle import law_cpu
+    meta, init, final = load(path)
+    ir = json.load(open(os.path.join(ROOT, "tests", "golden", "ir", meta["law"][:-4] + ".json")))
+    law = law_cpu.Law(ir)
+    s = law_cpu.Solver(law, tuple(meta["shape"]), meta["h"])
+    for k, v in init.items():
+        s.fields[k] = v.copy()
+    for _ in range(meta["steps"]):
+        s.step(meta["dt"])
+    assert s.substeps == meta["substeps"]
+    for name, want in final.items():
+        got = s.fields[name]
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (
+            f"{meta['name']}:{name} differs by {np.abs(got.astype(np.float64) - want).max()}")
+
+
+def test_heat_restatement_matches_the_law_oracle():
+    from oracle import heat as oh
+    from oracle import law_cpu
+    ir = json.load(open(os.path.join(ROOT, "tests", "golden", "ir", "heat.json")))
+    n, h = 20, 1.0 / 20
+    dt = 0.4 * h * h / 6.0
+    T0 = oh.gaussian_blobs(n, h, seed=5)
+    s = law_cpu.Solver(law_cpu.Law(ir), (n, n, n), h)
+    s.fields["T"] = T0.copy()
+    s.step(dt)
+    assert np.array_equal(s.fields["T"].view(np.uint32), oh.cpu_step(T0, 1.0, h, dt).view(np.uint32))
