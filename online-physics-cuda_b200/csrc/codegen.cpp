@@ -90,6 +90,11 @@ public:
 __device__ __forceinline__ int fe_ey(int v) { return v < 0 ? 0 : (v >= NY ? NY - 1 : v); }
 __device__ __forceinline__ int fe_ez(int v) { return v < 0 ? 0 : (v >= NZ ? NZ - 1 : v); }
 __device__ __forceinline__ bool fe_inside(int x, int y, int z) { return x >= 0 && y >= 0 && z >= 0 && x < NX && y < NY && z < NZ; }
+// IN: the cell and every point its expressions read lie inside the lattice (the pass checked its reach), so clamps are
+// the identity and edge tests are true; the same arithmetic, with the index work and the branches compiled away.
+template <bool IN> __device__ __forceinline__ int fe_cx(int v) { return IN ? v : fe_ex(v); }
+template <bool IN> __device__ __forceinline__ int fe_cy(int v) { return IN ? v : fe_ey(v); }
+template <bool IN> __device__ __forceinline__ int fe_cz(int v) { return IN ? v : fe_ez(v); }
 __device__ __forceinline__ int fe_imin(int a, int b) { return a < b ? a : b; }
 __device__ __forceinline__ int fe_imax(int a, int b) { return a > b ? a : b; }
 __device__ __forceinline__ void fe_run_to(int j, int d, int n, int& lo, int& hi)
@@ -227,14 +232,14 @@ private:
 
     static std::string v(int id, const std::string& x = "x", const std::string& y = "y", const std::string& z = "z")
     {
-        return "v" + std::to_string(id) + "(c, " + x + ", " + y + ", " + z + ")";
+        return "v" + std::to_string(id) + "<IN>(c, " + x + ", " + y + ", " + z + ")";
     }
 
     void emit_inst(std::ostringstream& f, PassBuild& pb, int id, bool body)
     {
         const Inst& in = at(id);
         const std::string name = (body ? "b" : "v") + std::to_string(id);
-        f << "template <class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)";
+        f << "template <bool IN, class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)";
         auto a = [&](std::size_t k, const std::string& x = "x", const std::string& y = "y", const std::string& z = "z") {
             return v(in.args[k], x, y, z);
         };
@@ -279,8 +284,8 @@ private:
             f << " { const float lo = " << a(1) << "; return fminf(fmaxf(" << a(0) << ", lo), fmaxf(lo, " << a(2) << ")); }\n";
             break;
         case Op::Shift:
-            simple(a(0, "fe_ex(x + " + std::to_string(in.offset[0]) + ")", "fe_ey(y + " + std::to_string(in.offset[1]) + ")",
-                "fe_ez(z + " + std::to_string(in.offset[2]) + ")"));
+            simple(a(0, "fe_cx<IN>(x + " + std::to_string(in.offset[0]) + ")", "fe_cy<IN>(y + " + std::to_string(in.offset[1]) + ")",
+                "fe_cz<IN>(z + " + std::to_string(in.offset[2]) + ")"));
             break;
         case Op::ShiftT:
             f << " { int lx, hx, ly, hy, lz, hz; fe_run_to(x, " << in.offset[0] << ", NX, lx, hx); fe_run_to(y, " << in.offset[1]
@@ -301,26 +306,26 @@ private:
             break;
         }
         case Op::Lap:
-            f << " { const float c0 = " << a(0) << "; return ((" << a(0, "fe_ex(x - 1)") << " - c0) + (" << a(0, "fe_ex(x + 1)")
-              << " - c0) + (" << a(0, "x", "fe_ey(y - 1)") << " - c0) + (" << a(0, "x", "fe_ey(y + 1)") << " - c0) + ("
-              << a(0, "x", "y", "fe_ez(z - 1)") << " - c0) + (" << a(0, "x", "y", "fe_ez(z + 1)") << " - c0)) / (FE_H * FE_H); }\n";
+            f << " { const float c0 = " << a(0) << "; return ((" << a(0, "fe_cx<IN>(x - 1)") << " - c0) + (" << a(0, "fe_cx<IN>(x + 1)")
+              << " - c0) + (" << a(0, "x", "fe_cy<IN>(y - 1)") << " - c0) + (" << a(0, "x", "fe_cy<IN>(y + 1)") << " - c0) + ("
+              << a(0, "x", "y", "fe_cz<IN>(z - 1)") << " - c0) + (" << a(0, "x", "y", "fe_cz<IN>(z + 1)") << " - c0)) / (FE_H * FE_H); }\n";
             break;
         case Op::Gx:
-            f << " { const int hi = fe_ex(x + 1); const int lo = fe_ex(x - 1); const int span = hi - lo; return span > 0 ? ("
+            f << " { const int hi = fe_cx<IN>(x + 1); const int lo = fe_cx<IN>(x - 1); const int span = hi - lo; return span > 0 ? ("
               << a(0, "hi") << " - " << a(0, "lo") << ") / (FE_H * span) : 0.f; }\n";
             break;
         case Op::Gy:
-            f << " { const int hi = fe_ey(y + 1); const int lo = fe_ey(y - 1); const int span = hi - lo; return span > 0 ? ("
+            f << " { const int hi = fe_cy<IN>(y + 1); const int lo = fe_cy<IN>(y - 1); const int span = hi - lo; return span > 0 ? ("
               << a(0, "x", "hi") << " - " << a(0, "x", "lo") << ") / (FE_H * span) : 0.f; }\n";
             break;
         case Op::Gz:
-            f << " { const int hi = fe_ez(z + 1); const int lo = fe_ez(z - 1); const int span = hi - lo; return span > 0 ? ("
+            f << " { const int hi = fe_cz<IN>(z + 1); const int lo = fe_cz<IN>(z - 1); const int span = hi - lo; return span > 0 ? ("
               << a(0, "x", "y", "hi") << " - " << a(0, "x", "y", "lo") << ") / (FE_H * span) : 0.f; }\n";
             break;
         case Op::Diffuse: {
-            static const char* sides[6][4] = {{"x > 0", "x - 1", "y", "z"}, {"x + 1 < NX", "x + 1", "y", "z"},
-                {"y > 0", "x", "y - 1", "z"}, {"y + 1 < NY", "x", "y + 1", "z"}, {"z > 0", "x", "y", "z - 1"},
-                {"z + 1 < NZ", "x", "y", "z + 1"}};
+            static const char* sides[6][4] = {{"IN || x > 0", "x - 1", "y", "z"}, {"IN || x + 1 < NX", "x + 1", "y", "z"},
+                {"IN || y > 0", "x", "y - 1", "z"}, {"IN || y + 1 < NY", "x", "y + 1", "z"}, {"IN || z > 0", "x", "y", "z - 1"},
+                {"IN || z + 1 < NZ", "x", "y", "z + 1"}};
             if (at(in.args[0]).shape == Shape::Scalar) {
                 // One k everywhere: the harmonic mean of a face is k itself (CudaCodegen.cpp:193-206).
                 f << " { const float c0 = " << a(1) << "; float acc = 0.f;\n";
@@ -337,8 +342,8 @@ private:
         }
         case Op::Adv: {
             auto up = [&](const std::string& speed, const char* pos, const char* count, const std::string& lo, const std::string& hi) {
-                return "(" + speed + " > 0.f ? (" + pos + " > 0 ? " + speed + " * (c0 - " + lo + ") / FE_H : 0.f) : (" + pos + " + 1 < " +
-                    count + " ? " + speed + " * (" + hi + " - c0) / FE_H : 0.f))";
+                return "(" + speed + " > 0.f ? ((IN || " + pos + " > 0) ? " + speed + " * (c0 - " + lo + ") / FE_H : 0.f) : ((IN || " + pos +
+                    " + 1 < " + count + ") ? " + speed + " * (" + hi + " - c0) / FE_H : 0.f))";
             };
             f << " { const float c0 = " << a(0) << "; const float u = " << a(1) << "; const float w = " << a(2) << "; const float s = " << a(3)
               << ";\n    return -(" << up("u", "x", "NX", a(0, "x - 1"), a(0, "x + 1")) << " + "
@@ -349,49 +354,49 @@ private:
         case Op::Fall: {
             const std::string n = std::to_string(id);
             f << ";\n";
-            f << "template <class C> __device__ __forceinline__ float fall" << n << "(const C& c, int x, int y, int z) { if (z == 0) return 0.f;\n"
+            f << "template <bool IN, class C> __device__ __forceinline__ float fall" << n << "(const C& c, int x, int y, int z) { if (!IN && z == 0) return 0.f;\n"
               << "    return fmaxf(0.f, " << a(2) << ") / FE_H * fmaxf(0.f, " << a(0) << ") * fe_sat(1.f - " << a(1, "x", "y", "z - 1")
               << " - " << a(0, "x", "y", "z - 1") << "); }\n";
-            f << "template <class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)"
-              << " { float o = -fall" << n << "(c, x, y, z); if (z + 1 < NZ) o += fall" << n << "(c, x, y, z + 1); return o; }\n";
+            f << "template <bool IN, class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)"
+              << " { float o = -fall" << n << "<IN>(c, x, y, z); if (IN || z + 1 < NZ) o += fall" << n << "<IN>(c, x, y, z + 1); return o; }\n";
             break;
         }
         case Op::Spread: {
             const std::string n = std::to_string(id);
             f << ";\n";
-            f << "template <class C> __device__ __forceinline__ float spread" << n << "(const C& c, int ax, int ay, int az, int bx, int by, int bz) {\n"
+            f << "template <bool IN, class C> __device__ __forceinline__ float spread" << n << "(const C& c, int ax, int ay, int az, int bx, int by, int bz) {\n"
               << "    const float fa = " << a(0, "ax", "ay", "az") << "; const float fb = " << a(0, "bx", "by", "bz") << ";\n"
               << "    const bool to_b = fa > fb; const int rx = to_b ? bx : ax; const int ry = to_b ? by : ay; const int rz = to_b ? bz : az;\n"
               << "    return 0.5f * (fmaxf(0.f, " << a(2, "ax", "ay", "az") << ") + fmaxf(0.f, " << a(2, "bx", "by", "bz")
               << ")) / (FE_H * FE_H) * (fa - fb) * fe_sat(1.f - " << a(1, "rx", "ry", "rz") << " - " << a(0, "rx", "ry", "rz") << "); }\n";
-            f << "template <class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)"
+            f << "template <bool IN, class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)"
               << " { float o = 0.f;\n"
-              << "    if (y > 0) o += spread" << n << "(c, x, y - 1, z, x, y, z);\n"
-              << "    if (x > 0) o += spread" << n << "(c, x - 1, y, z, x, y, z);\n"
-              << "    if (x + 1 < NX) o -= spread" << n << "(c, x, y, z, x + 1, y, z);\n"
-              << "    if (y + 1 < NY) o -= spread" << n << "(c, x, y, z, x, y + 1, z);\n"
+              << "    if (IN || y > 0) o += spread" << n << "<IN>(c, x, y - 1, z, x, y, z);\n"
+              << "    if (IN || x > 0) o += spread" << n << "<IN>(c, x - 1, y, z, x, y, z);\n"
+              << "    if (IN || x + 1 < NX) o -= spread" << n << "<IN>(c, x, y, z, x + 1, y, z);\n"
+              << "    if (IN || y + 1 < NY) o -= spread" << n << "<IN>(c, x, y, z, x, y + 1, z);\n"
               << "    return o; }\n";
             break;
         }
         case Op::Topple: {
             const std::string n = std::to_string(id);
             f << ";\n";
-            f << "template <class C> __device__ __forceinline__ float room" << n << "(const C& c, int x, int y, int z) { return fe_sat(1.f - " << a(1)
+            f << "template <bool IN, class C> __device__ __forceinline__ float room" << n << "(const C& c, int x, int y, int z) { return fe_sat(1.f - " << a(1)
               << " - " << a(0) << "); }\n"
-              << "template <class C> __device__ __forceinline__ float send" << n << "(const C& c, int x, int y, int z, int sx, int sy) {\n"
-              << "    const float here = " << a(0) << "; if (here <= 0.f || z == 0) return 0.f;\n"
-              << "    if (room" << n << "(c, x, y, z - 1) > 0.01f) return 0.f;\n"
-              << "    const int jx = x + sx; const int jy = y + sy; if (!fe_inside(jx, jy, z)) return 0.f;\n"
-              << "    return 0.25f * fmaxf(0.f, " << a(2) << ") / FE_H * here * fminf(room" << n << "(c, jx, jy, z), room" << n << "(c, jx, jy, z - 1)); }\n";
-            f << "template <class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)"
+              << "template <bool IN, class C> __device__ __forceinline__ float send" << n << "(const C& c, int x, int y, int z, int sx, int sy) {\n"
+              << "    const float here = " << a(0) << "; if (here <= 0.f || (!IN && z == 0)) return 0.f;\n"
+              << "    if (room" << n << "<IN>(c, x, y, z - 1) > 0.01f) return 0.f;\n"
+              << "    const int jx = x + sx; const int jy = y + sy; if (!IN && !fe_inside(jx, jy, z)) return 0.f;\n"
+              << "    return 0.25f * fmaxf(0.f, " << a(2) << ") / FE_H * here * fminf(room" << n << "<IN>(c, jx, jy, z), room" << n << "<IN>(c, jx, jy, z - 1)); }\n";
+            f << "template <bool IN, class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)"
               << " { float o = 0.f;\n"
-              << "    o -= send" << n << "(c, x, y, z, -1, 0); o -= send" << n << "(c, x, y, z, 1, 0); o -= send" << n << "(c, x, y, z, 0, -1); o -= send"
-              << n << "(c, x, y, z, 0, 1);\n"
-              << "    if (z + 1 < NZ) {\n"
-              << "        if (x + 1 < NX) o += send" << n << "(c, x + 1, y, z + 1, -1, 0);\n"
-              << "        if (x > 0) o += send" << n << "(c, x - 1, y, z + 1, 1, 0);\n"
-              << "        if (y + 1 < NY) o += send" << n << "(c, x, y + 1, z + 1, 0, -1);\n"
-              << "        if (y > 0) o += send" << n << "(c, x, y - 1, z + 1, 0, 1);\n"
+              << "    o -= send" << n << "<IN>(c, x, y, z, -1, 0); o -= send" << n << "<IN>(c, x, y, z, 1, 0); o -= send" << n << "<IN>(c, x, y, z, 0, -1); o -= send"
+              << n << "<IN>(c, x, y, z, 0, 1);\n"
+              << "    if (IN || z + 1 < NZ) {\n"
+              << "        if (IN || x + 1 < NX) o += send" << n << "<IN>(c, x + 1, y, z + 1, -1, 0);\n"
+              << "        if (IN || x > 0) o += send" << n << "<IN>(c, x - 1, y, z + 1, 1, 0);\n"
+              << "        if (IN || y + 1 < NY) o += send" << n << "<IN>(c, x, y + 1, z + 1, 0, -1);\n"
+              << "        if (IN || y > 0) o += send" << n << "<IN>(c, x, y - 1, z + 1, 0, 1);\n"
               << "    }\n    return o; }\n";
             break;
         }
@@ -439,6 +444,14 @@ private:
         fn("pl", pl);
         fn("base", base);
         f << "    static constexpr unsigned BYTES = " << bytes << "u;\n";
+        // The pass's true reach along each axis (unrounded): a cell this far from every face is interior (IN).
+        int rxt = 0, ryt = 0, rzt = 0;
+        for (const Radius& r : pb.reach) {
+            rxt = std::max(rxt, r.x);
+            ryt = std::max(ryt, r.y);
+            rzt = std::max(rzt, r.z);
+        }
+        f << "    static constexpr int RXT = " << rxt << ", RYT = " << ryt << ", RZT = " << rzt << ";\n";
         f << "    static __device__ __forceinline__ constexpr bool checked(int j) { ";
         for (int j = 0; j < nout; ++j) f << "if (j == " << j << ") return " << (checked[static_cast<std::size_t>(j)] ? "true" : "false") << "; ";
         f << "return false; }\n";
@@ -458,9 +471,11 @@ private:
         for (const Source& s : pb.sources) {
             if (128 + 2 * s.ax > 256 || s.ry > 64) return false;
         }
+        // The ring depth is a power of two (the ring position of a plane is a mask, not a division), at least 2 RZ + 2.
+        int least = 4;
+        while (least < 2 * rz + 2) least *= 2;
         for (const int ty : {16, 8}) {
-            for (int extra = 2; extra >= 0; --extra) {
-                const int nst = 2 * rz + 2 + extra;
+            for (const int nst : {2 * least, least}) {
                 std::size_t floats = 0;
                 for (const Source& s : pb.sources) {
                     const int plane = ((128 + 2 * s.ax) * (ty + 2 * s.ry) + 31) / 32 * 32;
@@ -532,11 +547,11 @@ private:
         }
         emit_traits(f, pb, L, static_cast<int>(outs.size()), checked);
         // The cell: every output's value, and the value it replaces (for the contracts).
-        f << "    template <class C> static __device__ __forceinline__ void cell(const C& c, int x, int y, int z, float* o, float* b) {\n";
+        f << "    template <bool IN, class C> static __device__ __forceinline__ void cell(const C& c, int x, int y, int z, float* o, float* b) {\n";
         for (std::size_t j = 0; j < outs.size(); ++j) {
             const PassOut& o = outs[j];
             if (o.kind == PassOut::StageBody) {
-                f << "        o[" << j << "] = b" << o.stage << "(c, x, y, z); b[" << j << "] = 0.f;\n";
+                f << "        o[" << j << "] = b" << o.stage << "<IN>(c, x, y, z); b[" << j << "] = 0.f;\n";
                 continue;
             }
             const int k = source_index(pb, Buf{Buf::FieldNow, o.target});
@@ -591,8 +606,9 @@ private:
         L.checked_fields = {-1, -1};
         emit_traits(f, pb, L, 2, {0, 0});
         f << "    template <class C> static __device__ __forceinline__ void coef(const C& c, int x, int y, int z, float& lo, float& di, float& up, float& rhs) {\n"
+          << "        constexpr bool IN = false;\n"
           << "        lo = " << v(in.args[0]) << "; up = " << v(in.args[2]) << "; di = " << v(in.args[1]) << "; rhs = " << v(in.args[3]) << ";\n    }\n";
-        f << "    template <class C> static __device__ __forceinline__ void cell(const C&, int, int, int, float*, float*) {}\n";
+        f << "    template <bool IN, class C> static __device__ __forceinline__ void cell(const C&, int, int, int, float*, float*) {}\n";
         f << "};\n}\n";
         L.kernel = "fe_tri_" + tag;
         if (in.index == 0) {
@@ -626,8 +642,9 @@ private:
         L.uniform = plan_.uniform_of[static_cast<std::size_t>(id)];
         emit_traits(f, pb, L, 0, {});
         f << "    static constexpr int KIND = " << (in.op == Op::SumOf ? 0 : (in.op == Op::MaxOf ? 1 : 2)) << ";\n"
-          << "    template <class C> static __device__ __forceinline__ float value(const C& c, int x, int y, int z) { return " << v(in.args[0]) << "; }\n"
-          << "    template <class C> static __device__ __forceinline__ void cell(const C&, int, int, int, float*, float*) {}\n"
+          << "    template <class C> static __device__ __forceinline__ float value(const C& c, int x, int y, int z) { constexpr bool IN = false; return "
+          << v(in.args[0]) << "; }\n"
+          << "    template <bool IN, class C> static __device__ __forceinline__ void cell(const C&, int, int, int, float*, float*) {}\n"
           << "};\n}\n";
         L.kernel = "fe_red_" + tag;
         f << "extern \"C\" __global__ void __launch_bounds__(256) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_reduce_pass<" << ns

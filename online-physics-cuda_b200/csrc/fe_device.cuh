@@ -198,24 +198,27 @@ __device__ __forceinline__ void fe_acc_row4(FeAcc& a, const float* before, const
         a.before += static_cast<double>((before[0] + before[1]) + (before[2] + before[3]));
         a.before_abs += static_cast<double>((fabsf(before[0]) + fabsf(before[1])) + (fabsf(before[2]) + fabsf(before[3])));
     }
+    const float s4 = (after[0] + after[1]) + (after[2] + after[3]);
     if (totals_after) {
-        a.after += static_cast<double>((after[0] + after[1]) + (after[2] + after[3]));
+        a.after += static_cast<double>(s4);
         a.after_abs += static_cast<double>((fabsf(after[0]) + fabsf(after[1])) + (fabsf(after[2]) + fabsf(after[3])));
     }
     if (range) {
-        a.lo = fminf(a.lo, fminf(fminf(after[0], after[1]), fminf(after[2], after[3])));
-        a.hi = fmaxf(a.hi, fmaxf(fmaxf(after[0], after[1]), fmaxf(after[2], after[3])));
-    }
-    const bool ok = !range || ((after[0] >= lo && after[0] <= hi) && (after[1] >= lo && after[1] <= hi) &&
-        (after[2] >= lo && after[2] <= hi) && (after[3] >= lo && after[3] <= hi));
-    if (!ok) {
+        // The group's least and most (NaN ignored) give the bounds and the range test at once; a NaN or an infinity
+        // anywhere makes the group's sum non-finite. Only a group that fails is looked at cell by cell.
+        const float mn = fminf(fminf(after[0], after[1]), fminf(after[2], after[3]));
+        const float mx = fmaxf(fmaxf(after[0], after[1]), fmaxf(after[2], after[3]));
+        a.lo = fminf(a.lo, mn);
+        a.hi = fmaxf(a.hi, mx);
+        if (!(mn >= lo && mx <= hi && fabsf(s4) <= 3.0e38f)) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            if (!(after[q] >= lo && after[q] <= hi)) fe_acc_bad(a, after[q], index0 + q);
+            for (int q = 0; q < 4; ++q) {
+                if (!(after[q] >= lo && after[q] <= hi)) fe_acc_bad(a, after[q], index0 + q);
+            }
         }
     }
-    a.changed |= ((__float_as_uint(before[0]) != __float_as_uint(after[0])) | (__float_as_uint(before[1]) != __float_as_uint(after[1])) |
-                     (__float_as_uint(before[2]) != __float_as_uint(after[2])) | (__float_as_uint(before[3]) != __float_as_uint(after[3])))
+    a.changed |= ((__float_as_uint(before[0]) ^ __float_as_uint(after[0])) | (__float_as_uint(before[1]) ^ __float_as_uint(after[1])) |
+                     (__float_as_uint(before[2]) ^ __float_as_uint(after[2])) | (__float_as_uint(before[3]) ^ __float_as_uint(after[3]))) != 0u
         ? 1u : 0u;
 }
 
@@ -358,13 +361,14 @@ __device__ __forceinline__ void fe_acc_finish(const double* partials, int blocks
 template <class P>
 struct FeSlabCtx {
     const float* sm;
-    int st[2 * P::RZ + 1];
+    int slot;      // the ring stage holding plane z (NST is a power of two: a neighbour plane's stage is a mask away)
     int x0, y0, z;
     float dt;
     template <int k>
     __device__ __forceinline__ float ld(int X, int Y, int Z) const
     {
-        return sm[P::base(k) + st[Z - z + P::RZ] * P::pl(k) + (Y - y0 + P::ry(k)) * P::px(k) + (X - x0 + P::ax(k))];
+        const int s = (slot + (Z - z)) & (P::NST - 1);
+        return sm[P::base(k) + s * P::pl(k) + (Y - y0 + P::ry(k)) * P::px(k) + (X - x0 + P::ax(k))];
     }
 };
 
@@ -452,16 +456,23 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         c.y0 = y0;
         c.z = z;
         c.dt = a.dt;
-#pragma unroll
-        for (int d = -P::RZ; d <= P::RZ; ++d) c.st[d + P::RZ] = (min(max(z + d, 0), P::NZ - 1) - zlo) % P::NST;
+        c.slot = (z - zlo) & (P::NST - 1);
+        const bool zin = z - P::RZT >= 0 && z + P::RZT < P::NZ;
 #pragma unroll
         for (int r = 0; r < P::R; ++r) {
             const int y = y0 + warp * P::R + r;
             if (y >= P::NY || x >= P::NX) continue;
             float o[4][P::NOUT];
             float b[4][P::NOUT];
+            // Four cells whose whole reach is inside the lattice take the clamp-free code; the rest the clamped one.
+            const bool in = zin && x - P::RXT >= 0 && x + 3 + P::RXT < P::NX && y - P::RYT >= 0 && y + P::RYT < P::NY;
+            if (in) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) P::cell(c, x + q, y, z, o[q], b[q]);
+                for (int q = 0; q < 4; ++q) P::template cell<true>(c, x + q, y, z, o[q], b[q]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) P::template cell<false>(c, x + q, y, z, o[q], b[q]);
+            }
             const fe_u64 at = static_cast<fe_u64>(x) + static_cast<fe_u64>(P::NX) * (static_cast<fe_u64>(y) + static_cast<fe_u64>(P::NY) * z);
 #pragma unroll
             for (int j = 0; j < P::NOUT; ++j) {
@@ -512,7 +523,7 @@ __device__ __forceinline__ void fe_plain_pass(const FePassArgs& a)
     for (int z = zb; live && z < ze; ++z) {
         float o[P::NOUT];
         float b[P::NOUT];
-        P::cell(c, x, y, z, o, b);
+        P::template cell<false>(c, x, y, z, o, b);
         const fe_u64 at = static_cast<fe_u64>(x) + static_cast<fe_u64>(P::NX) * (static_cast<fe_u64>(y) + static_cast<fe_u64>(P::NY) * z);
 #pragma unroll
         for (int j = 0; j < P::NOUT; ++j) {

@@ -73,8 +73,9 @@ def test_contracts_fused(cuda):
         rec = kernels.check_read(ws)
         s0, m0 = oh.totals(T0)
         s1, m1 = oh.totals(want)
-        assert rec.before == pytest.approx(s0, rel=1e-13) and rec.before_abs == pytest.approx(m0, rel=1e-13)
-        assert rec.after == pytest.approx(s1, rel=1e-13) and rec.after_abs == pytest.approx(m1, rel=1e-13)
+        # FP64 totals of fp32 sums of 4 cells: within a few 1e-8 of the exact total, far inside the contract's 1e-5.
+        assert rec.before == pytest.approx(s0, rel=1e-7) and rec.before_abs == pytest.approx(m0, rel=1e-7)
+        assert rec.after == pytest.approx(s1, rel=1e-7) and rec.after_abs == pytest.approx(m1, rel=1e-7)
         lib = _lib.lib()
         assert np.float32(lib.fe_key_to_float(~rec.lo_inv & 0xFFFFFFFF)) == want.min()
         assert np.float32(lib.fe_key_to_float(rec.hi_key)) == want.max()
