@@ -42,7 +42,7 @@ typedef struct fe_check {
     double before;      /* sum of the field before the term (FP64, fixed order) */
     double before_abs;  /* sum of |field| before the term */
     double after;       /* sum after the term */
-    double after_abs;
+    double after_abs;   /* 0: the fused passes do not keep it (the judge scales by before_abs) */
     uint32_t out_of_range;
     uint32_t not_finite;
     uint32_t first_bad; /* ~(linear index of the first bad cell); 0 if none */

@@ -56,15 +56,6 @@ MapCache& map_cache()
 
 constexpr std::size_t kCheckHeader = 128; // fe_check (64 bytes), error word, block counter, padding
 
-// 1/v when v is a power of two whose reciprocal is a normal float (then x / v == x * (1/v) to the bit), else 0.
-float exact_reciprocal(float v)
-{
-    int e = 0;
-    const float m = std::frexp(v, &e);
-    if (!(v > 0.0f) || m != 0.5f) return 0.0f;
-    const float r = 1.0f / v;
-    return std::isnormal(r) ? r : 0.0f;
-}
 
 } // namespace
 

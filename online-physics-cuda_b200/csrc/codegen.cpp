@@ -471,25 +471,68 @@ private:
         for (const Source& s : pb.sources) {
             if (128 + 2 * s.ax > 256 || s.ry > 64) return false;
         }
-        // The ring depth is a power of two (the ring position of a plane is a mask, not a division), at least 2 RZ + 2.
-        int least = 4;
-        while (least < 2 * rz + 2) least *= 2;
-        for (const int ty : {16, 8}) {
-            for (const int nst : {2 * least, least}) {
-                std::size_t floats = 0;
-                for (const Source& s : pb.sources) {
-                    const int plane = ((128 + 2 * s.ax) * (ty + 2 * s.ry) + 31) / 32 * 32;
-                    floats += static_cast<std::size_t>(plane) * nst;
-                }
-                if (floats * 4 <= 190 * 1024 && ty + 2 * rz < 256) {
-                    L.ty = ty;
-                    L.nst = nst;
-                    L.smem = static_cast<unsigned>(floats * 4);
-                    return true;
+        // The ring holds the 2 RZ + 1 planes a z reads and at least one being fetched; deeper rings fetch further ahead.
+        // Prefer the deepest ring that still leaves room for 3 CTAs an SM, then 2, then 1.
+        for (const std::size_t budget : {72u * 1024, 110u * 1024, 200u * 1024}) {
+            for (const int ty : {16, 8}) {
+                for (int nst = 2 * rz + 4; nst >= 2 * rz + 2; --nst) {
+                    std::size_t floats = 0;
+                    for (const Source& s : pb.sources) {
+                        const int plane = ((128 + 2 * s.ax) * (ty + 2 * s.ry) + 31) / 32 * 32;
+                        floats += static_cast<std::size_t>(plane) * nst;
+                    }
+                    if (floats * 4 <= budget && ty + 2 * rz < 256) {
+                        L.ty = ty;
+                        L.nst = nst;
+                        L.smem = static_cast<unsigned>(floats * 4);
+                        return true;
+                    }
                 }
             }
         }
         return false;
+    }
+
+    // How far along x a value reads, everything it inlines included (a stage read by it is one load: 0).
+    int xreach(int id, bool body, std::map<std::pair<int, bool>, int>& memo)
+    {
+        const auto key = std::make_pair(id, body);
+        const auto found = memo.find(key);
+        if (found != memo.end()) return found->second;
+        const Inst& in = at(id);
+        int r = 0;
+        if ((body || !(m_.is_stage(id) || in.global)) && in.op != Op::Field) {
+            const int own = axis_radius(in).x;
+            for (const int a : in.args) r = std::max(r, own + xreach(a, false, memo));
+        }
+        memo.emplace(key, r);
+        return r;
+    }
+
+    // Whether the lattice's x edge can be met by filling the staged x halo with the edge cell (what a clamped read
+    // returns) and reading without clamps: true when every op that reads along x gives the same arithmetic either way
+    // (shift, lap, diffuse, adv: a face past the edge reads the cell itself, a difference of +-0) and reads only values
+    // with no x reach of their own (a nested x stencil evaluated past the edge would not be the clamped one).
+    bool xfill_safe(const std::vector<int>& roots, bool bodies)
+    {
+        std::map<std::pair<int, bool>, int> memo;
+        std::set<std::pair<int, bool>> seen;
+        bool safe = true;
+        std::function<void(int, bool)> visit = [&](int id, bool body) {
+            if (!safe || !seen.insert({id, body}).second) return;
+            const Inst& in = at(id);
+            if (!body && (m_.is_stage(id) || in.global)) return;
+            if (axis_radius(in).x > 0) {
+                const bool kind_ok = in.op == Op::Shift || in.op == Op::Lap || in.op == Op::Diffuse || in.op == Op::Adv;
+                if (!kind_ok) safe = false;
+                for (const int a : in.args) {
+                    if (xreach(a, false, memo) != 0) safe = false;
+                }
+            }
+            for (const int a : in.args) visit(a, false);
+        };
+        for (const int r : roots) visit(r, bodies);
+        return safe;
     }
 
     static constexpr std::size_t FE_MAX_SRC_HOST = 12;
@@ -546,6 +589,7 @@ private:
             L.nst = 4;
         }
         emit_traits(f, pb, L, static_cast<int>(outs.size()), checked);
+        f << "    static constexpr bool XFILL = " << (xfill_safe(roots, bodies) ? "true" : "false") << ";\n";
         // The cell: every output's value, and the value it replaces (for the contracts).
         f << "    template <bool IN, class C> static __device__ __forceinline__ void cell(const C& c, int x, int y, int z, float* o, float* b) {\n";
         for (std::size_t j = 0; j < outs.size(); ++j) {

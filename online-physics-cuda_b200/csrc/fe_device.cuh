@@ -191,6 +191,9 @@ __device__ __forceinline__ void fe_acc_bad(FeAcc& a, float after, unsigned index
 }
 
 // Four consecutive cells (index0 .. index0 + 3): their values before the pass and after it; lo/hi the declared range.
+// The sum of |after| is not kept (the judge scales its tolerance by the sum of |before|, Solver.cpp:439-453). With
+// BITS the change flag compares the cells' bits; without it the caller sets a.changed itself (from its increments).
+template <bool BITS = true>
 __device__ __forceinline__ void fe_acc_row4(FeAcc& a, const float* before, const float* after, float lo, float hi,
     unsigned index0, bool totals_before, bool totals_after, bool range = true)
 {
@@ -201,7 +204,6 @@ __device__ __forceinline__ void fe_acc_row4(FeAcc& a, const float* before, const
     const float s4 = (after[0] + after[1]) + (after[2] + after[3]);
     if (totals_after) {
         a.after += static_cast<double>(s4);
-        a.after_abs += static_cast<double>((fabsf(after[0]) + fabsf(after[1])) + (fabsf(after[2]) + fabsf(after[3])));
     }
     if (range) {
         // The group's least and most (NaN ignored) give the bounds and the range test at once; a NaN or an infinity
@@ -217,9 +219,11 @@ __device__ __forceinline__ void fe_acc_row4(FeAcc& a, const float* before, const
             }
         }
     }
-    a.changed |= ((__float_as_uint(before[0]) ^ __float_as_uint(after[0])) | (__float_as_uint(before[1]) ^ __float_as_uint(after[1])) |
-                     (__float_as_uint(before[2]) ^ __float_as_uint(after[2])) | (__float_as_uint(before[3]) ^ __float_as_uint(after[3]))) != 0u
-        ? 1u : 0u;
+    if (BITS) {
+        a.changed |= ((__float_as_uint(before[0]) ^ __float_as_uint(after[0])) | (__float_as_uint(before[1]) ^ __float_as_uint(after[1])) |
+                         (__float_as_uint(before[2]) ^ __float_as_uint(after[2])) | (__float_as_uint(before[3]) ^ __float_as_uint(after[3]))) != 0u
+            ? 1u : 0u;
+    }
 }
 
 // One cell (the plain passes).
@@ -232,7 +236,6 @@ __device__ __forceinline__ void fe_acc_cell(FeAcc& a, float before, float after,
     }
     if (totals_after) {
         a.after += static_cast<double>(after);
-        a.after_abs += static_cast<double>(fabsf(after));
     }
     if (range) {
         a.lo = fminf(a.lo, after);
@@ -361,16 +364,57 @@ __device__ __forceinline__ void fe_acc_finish(const double* partials, int blocks
 template <class P>
 struct FeSlabCtx {
     const float* sm;
-    int slot;      // the ring stage holding plane z (NST is a power of two: a neighbour plane's stage is a mask away)
+    int slots[2 * P::RZ + 1]; // the ring stage of plane z + d at slots[d + RZ]
     int x0, y0, z;
     float dt;
+    // The stage of plane Z (|Z - z| <= RZ): a chain of selects, so the table stays in registers whatever Z is.
+    __device__ __forceinline__ int stage(int Z) const
+    {
+        const int d = Z - z + P::RZ;
+        int s = slots[0];
+#pragma unroll
+        for (int i = 1; i < 2 * P::RZ + 1; ++i) s = d == i ? slots[i] : s;
+        return s;
+    }
     template <int k>
     __device__ __forceinline__ float ld(int X, int Y, int Z) const
     {
-        const int s = (slot + (Z - z)) & (P::NST - 1);
-        return sm[P::base(k) + s * P::pl(k) + (Y - y0 + P::ry(k)) * P::px(k) + (X - x0 + P::ax(k))];
+        return sm[P::base(k) + stage(Z) * P::pl(k) + (Y - y0 + P::ry(k)) * P::px(k) + (X - x0 + P::ax(k))];
     }
 };
+
+// For passes whose x edge the halo can carry (P::XFILL): after plane j lands, the staged columns past the lattice's x
+// edge get the edge cell's value, what a clamped read returns there. Only the CTAs at an x edge do anything; one row a
+// thread.
+template <class P>
+__device__ __forceinline__ void fe_fill_x_edges(float* sm, int j, int x0)
+{
+    if (!P::XFILL) return;
+    const bool left = x0 == 0;
+    const int inside = P::NX - x0; // columns of this tile inside the lattice
+    const bool right = x0 + 128 >= P::NX;
+    if (!left && !right) return;
+#pragma unroll
+    for (int k = 0; k < P::NSRC; ++k) {
+        const int ax = P::ax(k);
+        if (ax == 0) continue;
+        const int rows = P::W * P::R + 2 * P::ry(k);
+        const int px = P::px(k);
+        float* plane = sm + P::base(k) + (j % P::NST) * P::pl(k);
+        for (int row = threadIdx.x; row < rows; row += blockDim.x) {
+            float* r = plane + row * px;
+            if (left) {
+                const float edge = r[ax];
+                for (int c = 0; c < ax; ++c) r[c] = edge;
+            }
+            if (right) {
+                const int first_out = ax + min(inside, 128);
+                const float edge = r[first_out - 1];
+                for (int c = first_out; c < px; ++c) r[c] = edge;
+            }
+        }
+    }
+}
 
 // Global-memory reads (through the read-only path), for passes the TMA cannot stage (an x extent not a multiple of 4).
 template <class P>
@@ -440,15 +484,21 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
 #pragma unroll
     for (int j = 0; j < P::NOUT; ++j) fe_acc_init(acc[j]);
     int waited = 0;
+    // Every thread waits (bounded) for the planes a z needs, and evens the x edge of each plane that landed (XFILL); the
+    // barrier that follows makes both visible and the outcome uniform.
     auto wait_upto = [&](int j) {
         while (waited <= j) {
             if (!fe_mbar_wait(&bar[waited % P::NST], static_cast<unsigned>((waited / P::NST) & 1), 1u << 20)) failed = 1;
+            else fe_fill_x_edges<P>(fe_sm, waited, x0);
             ++waited;
         }
     };
     if (zb < ze) wait_upto(min(zb + P::RZ, P::NZ - 1) - zlo);
     __syncthreads();
     const int x = x0 + 4 * lane;
+    // With the x edge carried by the halo, whether a row's cells are interior depends only on the row and the plane, so
+    // a warp takes one path.
+    const bool xin = P::XFILL || (x - P::RXT >= 0 && x + 3 + P::RXT < P::NX);
     for (int z = zb; z < ze && !failed; ++z) {
         FeSlabCtx<P> c;
         c.sm = fe_sm;
@@ -456,7 +506,8 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         c.y0 = y0;
         c.z = z;
         c.dt = a.dt;
-        c.slot = (z - zlo) & (P::NST - 1);
+#pragma unroll
+        for (int d = -P::RZ; d <= P::RZ; ++d) c.slots[d + P::RZ] = (min(max(z + d, 0), P::NZ - 1) - zlo) % P::NST;
         const bool zin = z - P::RZT >= 0 && z + P::RZT < P::NZ;
 #pragma unroll
         for (int r = 0; r < P::R; ++r) {
@@ -465,7 +516,7 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
             float o[4][P::NOUT];
             float b[4][P::NOUT];
             // Four cells whose whole reach is inside the lattice take the clamp-free code; the rest the clamped one.
-            const bool in = zin && x - P::RXT >= 0 && x + 3 + P::RXT < P::NX && y - P::RYT >= 0 && y + P::RYT < P::NY;
+            const bool in = zin && xin && y - P::RYT >= 0 && y + P::RYT < P::NY;
             if (in) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) P::template cell<true>(c, x + q, y, z, o[q], b[q]);

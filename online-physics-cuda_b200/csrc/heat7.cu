@@ -34,7 +34,7 @@ struct HeatTile {
     static constexpr unsigned BOX_BYTES = PX * PY * 4u;
 };
 
-template <int W, int R, int NST>
+template <int W, int R, int NST, bool DIV>
 __global__ void __launch_bounds__(W * 32) heat7_tma(const __grid_constant__ FeTensorMap tin, const HeatArgs a)
 {
     using Tile = HeatTile<W, R>;
@@ -96,7 +96,14 @@ __global__ void __launch_bounds__(W * 32) heat7_tma(const __grid_constant__ FeTe
     const int px = kHeatPadX + 4 * lane;
     const int x = x0 + 4 * lane;
     const bool xin = x < nx;
+    const bool xm_ok = x > 0;       // this lane's first cell has a -x face
+    const bool xp_ok = x + 4 < nx;  // its last cell has a +x face (nx is a multiple of 4)
+    const bool before = a.totals_before != 0;
+    const bool after = a.totals_after != 0;
     for (int z = zb; z < ze && !failed; ++z) {
+        // A face past the lattice's edge reads the cell itself, so it adds (c - c) = +0, which leaves the sum as it is:
+        // the sum starts at +0 and a round-to-nearest sum of nonzero terms is never -0, so this and skipping the face
+        // agree to the bit. Along z the edge plane stands in for the missing one; along y, the row itself.
         const int jm = max(z - 1, 0) - zlo;
         const int jc = z - zlo;
         const int jp = min(z + 1, nz - 1) - zlo;
@@ -116,8 +123,12 @@ __global__ void __launch_bounds__(W * 32) heat7_tma(const __grid_constant__ FeTe
             if (!xin || y >= ny) {
                 continue;
             }
-            const float4 up = *reinterpret_cast<const float4*>(pc + row - Tile::PX + px);
-            const float4 dn = *reinterpret_cast<const float4*>(pc + row + Tile::PX + px);
+            left = xm_ok ? left : c.x;
+            right = xp_ok ? right : c.w;
+            const int row_up = y > 0 ? row - Tile::PX : row;
+            const int row_dn = y + 1 < ny ? row + Tile::PX : row;
+            const float4 up = *reinterpret_cast<const float4*>(pc + row_up + px);
+            const float4 dn = *reinterpret_cast<const float4*>(pc + row_dn + px);
             const float4 zm = *reinterpret_cast<const float4*>(pm + row + px);
             const float4 zp = *reinterpret_cast<const float4*>(pp + row + px);
             const float cv[4] = {c.x, c.y, c.z, c.w};
@@ -127,30 +138,30 @@ __global__ void __launch_bounds__(W * 32) heat7_tma(const __grid_constant__ FeTe
             const float yr[4] = {dn.x, dn.y, dn.z, dn.w};
             const float zl[4] = {zm.x, zm.y, zm.z, zm.w};
             const float zr[4] = {zp.x, zp.y, zp.z, zp.w};
-            const bool ym = y > 0, yp = y + 1 < ny, zmv = z > 0, zpv = z + 1 < nz;
             float o[4];
+            bool moved = false;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                // A face past the edge adds (c - c) = +0, which leaves the sum as it is: the sum starts at +0 and a
-                // round-to-nearest sum of nonzero terms is never -0, so skipping the face and adding +0 agree to the bit.
                 const float cc = cv[q];
                 float s = 0.f;
-                s = __fadd_rn(s, __fsub_rn(x + q > 0 ? xl[q] : cc, cc));
-                s = __fadd_rn(s, __fsub_rn(x + q + 1 < nx ? xr[q] : cc, cc));
-                s = __fadd_rn(s, __fsub_rn(ym ? yl[q] : cc, cc));
-                s = __fadd_rn(s, __fsub_rn(yp ? yr[q] : cc, cc));
-                s = __fadd_rn(s, __fsub_rn(zmv ? zl[q] : cc, cc));
-                s = __fadd_rn(s, __fsub_rn(zpv ? zr[q] : cc, cc));
+                s = __fadd_rn(s, __fsub_rn(xl[q], cc));
+                s = __fadd_rn(s, __fsub_rn(xr[q], cc));
+                s = __fadd_rn(s, __fsub_rn(yl[q], cc));
+                s = __fadd_rn(s, __fsub_rn(yr[q], cc));
+                s = __fadd_rn(s, __fsub_rn(zl[q], cc));
+                s = __fadd_rn(s, __fsub_rn(zr[q], cc));
                 const float ks = __fmul_rn(kk, s);
-                // (k s) / h^2: when h^2 is a power of two the host passes its exact reciprocal and the division is that
-                // multiplication, to the bit.
-                const float rate = a.inv_hh != 0.f ? __fmul_rn(ks, a.inv_hh) : __fdiv_rn(ks, hh);
+                // (k s) / h^2: when h^2 is a power of two its exact reciprocal multiplies instead, to the bit.
+                const float rate = DIV ? __fdiv_rn(ks, hh) : __fmul_rn(ks, a.inv_hh);
                 const float d = __fmul_rn(rate, a.dt);
                 o[q] = d != 0.f ? __fadd_rn(cc, d) : cc;
+                moved = moved || d != 0.f;
             }
             const size_t at = static_cast<size_t>(x) + static_cast<size_t>(nx) * (static_cast<size_t>(y) + static_cast<size_t>(ny) * z);
             if (check) {
-                fe_acc_row4(acc, cv, o, a.lo, a.hi, static_cast<unsigned>(at), a.totals_before != 0, a.totals_after != 0);
+                // The change flag as the reference's gather sets it: an increment that is not zero (CudaCodegen.cpp:598).
+                fe_acc_row4<false>(acc, cv, o, a.lo, a.hi, static_cast<unsigned>(at), before, after);
+                acc.changed |= moved ? 1u : 0u;
             }
             *reinterpret_cast<float4*>(a.out + at) = make_float4(o[0], o[1], o[2], o[3]);
         }
@@ -259,22 +270,28 @@ struct HeatShape {
     int W, R, NST, zchunk;
 };
 
-template <int W, int R, int NST>
-cudaError_t launch_heat7_tma_t(const FeTensorMap& map, const HeatArgs& a, cudaStream_t stream)
+template <int W, int R, int NST, bool DIV>
+cudaError_t launch_heat7_tma_d(const FeTensorMap& map, const HeatArgs& a, cudaStream_t stream)
 {
     using Tile = HeatTile<W, R>;
     const size_t smem = static_cast<size_t>(NST) * Tile::PLANE * sizeof(float);
     static bool configured = false;
     if (!configured) {
-        const cudaError_t e = cudaFuncSetAttribute(heat7_tma<W, R, NST>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        const cudaError_t e = cudaFuncSetAttribute(heat7_tma<W, R, NST, DIV>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) {
             return e;
         }
         configured = true;
     }
     const dim3 grid((a.nx + kHeatTX - 1) / kHeatTX, (a.ny + Tile::TY - 1) / Tile::TY, (a.nz + a.zchunk - 1) / a.zchunk);
-    heat7_tma<W, R, NST><<<grid, W * 32, smem, stream>>>(map, a);
+    heat7_tma<W, R, NST, DIV><<<grid, W * 32, smem, stream>>>(map, a);
     return cudaGetLastError();
+}
+
+template <int W, int R, int NST>
+cudaError_t launch_heat7_tma_t(const FeTensorMap& map, const HeatArgs& a, cudaStream_t stream)
+{
+    return a.inv_hh != 0.f ? launch_heat7_tma_d<W, R, NST, false>(map, a, stream) : launch_heat7_tma_d<W, R, NST, true>(map, a, stream);
 }
 
 // Tile rows (W warps x R rows) and ring depth: the shapes the autotuner may pick from.

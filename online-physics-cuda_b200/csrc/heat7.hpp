@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstddef>
 
 #include "fe_device.cuh"
@@ -23,6 +24,16 @@ struct HeatArgs {
     unsigned* count;    // blocks finished (reset by the last)
     unsigned* err;      // error word (bounded waits)
 };
+
+// 1/v when v is a power of two whose reciprocal is a normal float (then x / v == x * (1/v) to the bit), else 0.
+inline float exact_reciprocal(float v)
+{
+    int e = 0;
+    const float m = std::frexp(v, &e);
+    if (!(v > 0.0f) || m != 0.5f) return 0.0f;
+    const float r = 1.0f / v;
+    return std::isnormal(r) ? r : 0.0f;
+}
 
 cudaError_t launch_heat7_tma(int variant, const FeTensorMap& map, const HeatArgs& a, cudaStream_t stream);
 cudaError_t launch_heat7_plain(const float* T, const HeatArgs& a, cudaStream_t stream);
