@@ -78,6 +78,18 @@ int fe_check_read(const void* workspace, fe_check* out, void* stream);
 /* A device-to-device copy of n floats (n a multiple of 4, 16-byte aligned): the bandwidth roof for the roofline. */
 int fe_copy_f32(const float* src_dev, float* dst_dev, size_t n, void* stream);
 
+/* fe_heat7_step without a workspace, for callers that cannot allocate device memory (their device memory belongs to
+ * another allocator or pool, they are plugins in a process that forbids new device allocations, or they cannot afford
+ * cudaMalloc's synchronisation in their loop). It has no counterpart in the reference. The contract pass's per-block
+ * partial sums live in a fixed array in the library's device memory (every GPU that loads the library holds it, about
+ * 256 KiB, until exit), which limits a pass to 8192 thread blocks: larger lattices are refused with FE_EINVAL (raise
+ * zchunk). The caller passes the field buffers and, with `check`, a device fe_check `record_dev` that the call clears
+ * and fills (a kernel error word lands in record_dev->pad[0]). The array is shared by every call; each call clears
+ * what must start at zero, and calls that overlap on the GPU race on it. The first call on a device looks up the
+ * array's device address (once per device, with that device current). Nothing here calls cudaMalloc or cudaFree. */
+int fe_heat7_step_noalloc(const float* T_dev, float* out_dev, int nx, int ny, int nz, float k, float h, float dt, float lo,
+    float hi, int variant, int zchunk, int check, fe_check* record_dev, void* stream);
+
 /* ---- the law backend ------------------------------------------------------------------------------------------------
  * A law (the reference's .law text, unchanged) compiled for one lattice nx*ny*nz of cell size h: parsed, lowered to the
  * SSA IR with the reference's rules, turned into sm_100a kernels (NVRTC), with its fields on the card. The handle is

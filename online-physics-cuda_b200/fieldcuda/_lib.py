@@ -94,6 +94,9 @@ SIGNATURES = {
     "fe_check_reset": (_c.c_int, [_c.c_void_p, _c.c_void_p]),
     "fe_check_read": (_c.c_int, [_c.c_void_p, _c.POINTER(fe_check), _c.c_void_p]),
     "fe_copy_f32": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_size_t, _c.c_void_p]),
+    "fe_heat7_step_noalloc": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_int, _c.c_int, _c.c_int, _c.c_float, _c.c_float,
+                                         _c.c_float, _c.c_float, _c.c_float, _c.c_int, _c.c_int, _c.c_int, _c.c_void_p,
+                                         _c.c_void_p]),
     "fe_law_create": (_i, [_cs, _cs, _i, _i, _i, _d, _c.POINTER(_p)]),
     "fe_law_destroy": (None, [_p]),
     "fe_law_ir_json": (_i, [_cs, _p, _s, _c.POINTER(_s)]),
