@@ -201,10 +201,57 @@ def run_reference_arm(args, world, rank):
 
 # ---- our arm ---------------------------------------------------------------------------------------------------------
 
+def _events(stream):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    return e0, e1
+
+
+def handwritten_ms(n, h, dt, cells, stream, variant=0, zchunk=32, reps=10):
+    """The hand-written kernel (same arithmetic, contracts on): ms per step, for comparison."""
+    import torch
+    from fieldcuda import _lib, kernels
+    a = torch.rand((n, n, n), device="cuda")
+    b = torch.empty_like(a)
+    ws = kernels.heat7_workspace((n, n, n), variant, zchunk)
+    flags = dict(lo=-1e6, hi=1e6, variant=variant, zchunk=zchunk, check=_lib.FE_HEAT7_BEFORE | _lib.FE_HEAT7_AFTER)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            kernels.check_reset(ws, stream)
+            kernels.heat7_step(a, b, 1.0, h, dt, workspace=ws, stream=stream, **flags)
+        e0, e1 = _events(stream)
+        e0.record(stream)
+        for _ in range(reps):
+            kernels.check_reset(ws, stream)
+            kernels.heat7_step(a, b, 1.0, h, dt, workspace=ws, stream=stream, **flags)
+            a, b = b, a
+        e1.record(stream)
+        stream.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def copy_roof_gbs(cells, stream, reps=10):
+    import torch
+    from fieldcuda import kernels
+    ca = torch.empty(cells, dtype=torch.float32, device="cuda")
+    cb = torch.empty_like(ca)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            kernels.copy_f32(ca, cb, stream)
+        e0, e1 = _events(stream)
+        e0.record(stream)
+        for _ in range(reps):
+            kernels.copy_f32(ca, cb, stream)
+        e1.record(stream)
+        stream.synchronize()
+    return 2 * 4 * cells * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
-    from fieldcuda import _lib, kernels
+    from fieldcuda import _lib
+    from fieldcuda.solver import Solver
     from oracle import heat as oh
 
     torch.cuda.set_device(local)
@@ -213,96 +260,68 @@ def run_ours(args, world, rank, local):
     h = 1.0 / n
     dt = 0.4 * h * h / 6.0
     cells = n ** 3
-    variant, zchunk = args.variant, args.zchunk
-    stream = torch.cuda.Stream()
-    T0 = oh.gaussian_blobs(n, h, seed=rank)
-    host = torch.from_numpy(T0).pin_memory()
-    a = torch.empty((n, n, n), dtype=torch.float32, device="cuda")
-    b = torch.empty_like(a)
     K, W = args.steps, args.warmup
-    # One workspace (contract record + per-block partials) per timed step: records are judged after the run, so no
-    # step waits on the host.
-    ws = [kernels.heat7_workspace((n, n, n), variant, zchunk) for _ in range(max(K, W))]
-    check = _lib.FE_HEAT7_BEFORE | _lib.FE_HEAT7_AFTER
-    flags = dict(lo=-1e6, hi=1e6, variant=variant, zchunk=zchunk, check=check)
+    T0 = oh.gaussian_blobs(n, h, seed=rank)
+    pinned_in = torch.from_numpy(T0).pin_memory()
+    pinned_out = torch.empty((n, n, n), dtype=torch.float32).pin_memory()
 
-    with torch.cuda.stream(stream):
-        a.copy_(host, non_blocking=True)
-        for i in range(W):
-            kernels.check_reset(ws[i], stream)
-            kernels.heat7_step(a, b, 1.0, h, dt, workspace=ws[i], stream=stream, **flags)
-            a, b = b, a
-        stream.synchronize()
+    # The product path: the law compiled by the backend (IR -> sm_100a kernels), stepped through the C ABI.
+    s = Solver(HEAT_LAW, n, n, n, h, "heat.law")
+    s.set_field("T", pinned_in.numpy())
+    stream = torch.cuda.ExternalStream(s.stream)
+    s.set_deferred(True)  # contracts checked every step, judged after the run: no step waits for the host
+    for _ in range(W):
+        s.step(dt)
+    s.sync()
+    assert not s.violations(), s.violations()
 
-        # Copy roof in the same run: a device-to-device copy of the same bytes.
-        ca = torch.empty(cells, dtype=torch.float32, device="cuda")
-        cb = torch.empty_like(ca)
-        for _ in range(3):
-            kernels.copy_f32(ca, cb, stream)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(10):
-            kernels.copy_f32(ca, cb, stream)
-        e1.record(stream)
-        stream.synchronize()
-        copy_gbs = 2 * 4 * cells * 10 / (e0.elapsed_time(e1) * 1e-3) / 1e9
-        del ca, cb
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = _events(stream)
+    e0.record(stream)
+    launches = 0
+    for _ in range(K):
+        s.step(dt)
+        launches += s.profile()["launches"]
+    e1.record(stream)
+    stream.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms_total = max_over_ranks(world, e0.elapsed_time(e1))
+    s.sync()  # judge every timed step's contracts (conserved total, range, NaN)
+    broken = s.violations()
+    assert not broken, broken
 
-        clocks = ClockSampler(torch.cuda.current_device())
-        clocks.start()
-        barrier(world)
-        torch.cuda.synchronize()
-        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        start.record(stream)
-        for i in range(K):
-            kernels.check_reset(ws[i], stream)
-            kernels.heat7_step(a, b, 1.0, h, dt, workspace=ws[i], stream=stream, **flags)
-            a, b = b, a
-        end.record(stream)
-        stream.synchronize()
-        torch.cuda.synchronize()
-        barrier(world)
-        clk = clocks.stop()
-        ms_total = start.elapsed_time(end)
-        ms_total = max_over_ranks(world, ms_total)
-        recs = [kernels.check_read(ws[i], stream) for i in range(K)]
-        # Judge the conserved-total contract of every timed step (Solver.cpp:439-453's tolerance).
-        worst = 0.0
-        for r in recs:
-            tol = 1e-5 * (r.before_abs + 1.0)
-            worst = max(worst, abs(r.after - r.before) / tol)
-            assert r.out_of_range == 0 and r.not_finite == 0
-        assert worst <= 1.0, f"conservation broken: {worst}"
+    # The dominant kernel alone: the generated gather pass (one launch a step), timed back to back.
+    gather_ms = max_over_ranks(world, s.time_gather(0, 20) / 20)
 
-        # End to end through the C ABI with host buffers: the initial state up from pinned host memory, K steps, each
-        # step's contract record read back to the host, the final state back down.
-        rec_host = torch.empty((K, 128), dtype=torch.uint8).pin_memory()
-        out_host = torch.empty((n, n, n), dtype=torch.float32).pin_memory()
-        barrier(world)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        e2 = torch.cuda.Event(enable_timing=True)
-        e3 = torch.cuda.Event(enable_timing=True)
-        e2.record(stream)
-        a.copy_(host, non_blocking=True)
-        for i in range(K):
-            kernels.check_reset(ws[i], stream)
-            kernels.heat7_step(a, b, 1.0, h, dt, workspace=ws[i], stream=stream, **flags)
-            rec_host[i].copy_(ws[i][:128], non_blocking=True)
-            a, b = b, a
-        out_host.copy_(a, non_blocking=True)
-        e3.record(stream)
-        stream.synchronize()
-        e2e_ms = max_over_ranks(world, e2.elapsed_time(e3))
-        wall_e2e_ms = (time.perf_counter() - t0) * 1e3
+    # End to end through the public API with host buffers: the state up from pinned host memory, K steps each judged
+    # on the host (its contract records read back), the state back down to pinned host memory.
+    s.set_deferred(False)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.set_field("T", pinned_in.numpy())
+    for _ in range(K):
+        s.step(dt)
+    _lib.check(_lib.lib().fe_law_fetch(s._h, 0, ctypes.c_void_p(pinned_out.data_ptr())))
+    e2e_ms = max_over_ranks(world, (time.perf_counter() - t0) * 1e3)
+    assert not s.violations(), s.violations()
+    s.close()
+
+    side = torch.cuda.Stream()
+    hand_ms = handwritten_ms(n, h, dt, cells, side)
+    copy_gbs = copy_roof_gbs(cells, side)
 
     ms_step = ms_total / K
     total_cells = cells * world
     value = BYTES_PER_CELL * total_cells * K / (ms_total * 1e-3) / 1e9
     e2e_value = BYTES_PER_CELL * total_cells * K / (e2e_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
-    per_launch_achieved = BYTES_PER_CELL * cells / (ms_step * 1e-3) / 1e9
-    traffic = profile_traffic("heat7_tma_512.md")
+    achieved = BYTES_PER_CELL * cells / (gather_ms * 1e-3) / 1e9
+    traffic = profile_traffic("heat_gather_512.md")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -311,7 +330,7 @@ def run_ours(args, world, rank, local):
         if res is not None:
             ms, kind, cores = res
             cpu = {"value": BYTES_PER_CELL * cells / (ms * 1e-3) / 1e9, "unit": "GB/s", "cores": cores, "kind": kind,
-                   "sample": f"2 timed steps of the {n}^3 heat law after 1 warm-up (reference lawc, its OpenMP solver)"}
+                   "sample": f"2 timed steps of the {n}^3 heat law after 1 warm-up (the reference's lawc, its OpenMP solver)"}
         else:
             t = time.perf_counter()
             oh.cpu_step(T0, 1.0, h, dt)
@@ -326,18 +345,21 @@ def run_ours(args, world, rank, local):
         "value": value, "unit": "GB/s", "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: sum of 4 seeded Gaussian blobs (numpy default_rng(rank))",
-        "config": {"workload": f"heat 7-pt diffuse(D=1,T) {n}^3 fp32, conserves T, 1 substep, contracts fused and "
-                               f"judged for every step", "cells_per_gpu": cells, "kernel": f"heat7_tma variant {variant}",
-                   "zchunk": zchunk, "l2": "inputs larger than L2 (512 MiB a buffer)"},
-        "roofline": {"bound": "hbm", "achieved": per_launch_achieved, "peak": peak, "unit": "GB/s",
-                     "frac": per_launch_achieved / peak, "traffic": traffic,
+        "config": {"workload": f"heat law d T = diffuse(1, T), conserves T, {n}^3 fp32, h = 1/{n}, dt = 0.4 h^2/6 "
+                               f"(1 substep), contracts checked every step", "cells_per_gpu": cells,
+                   "path": "fe_law_step (law text -> IR -> generated sm_100a TMA pass)",
+                   "l2": "inputs larger than L2 (512 MiB a buffer)",
+                   "handwritten_kernel_gbs": BYTES_PER_CELL * cells / (hand_ms * 1e-3) / 1e9},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "generated gather pass fe_pass_t0g (8 B/cell)",
                      "peak_source": f"{peak_kind} copy (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                      "copy_same_run_gbs": copy_gbs},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": 4 * cells // K,
-                "d2h_bytes_per_step": 128 + 4 * cells // K, "wall_ms": wall_e2e_ms,
-                "what": "initial state H2D from pinned host, K steps, each step's contract record D2H, final state D2H"},
-        "gpu_launches": K,
+                "d2h_bytes_per_step": 64 + 4 + 4 * cells // K, "ms": e2e_ms,
+                "what": "fe_law_upload of the state from pinned host memory, K fe_law_step each judged on the host, "
+                        "fe_law_fetch of the state to pinned host memory (wall clock)"},
+        "gpu_launches": launches,
         "clocks": clk,
     }))
 
@@ -349,8 +371,6 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=512)
-    ap.add_argument("--variant", type=int, default=0)
-    ap.add_argument("--zchunk", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     world, rank, local = init_dist()

@@ -199,13 +199,14 @@ CUfunction Engine::function(const std::string& name, unsigned smem, std::string&
 
 int Engine::zchunk_for(const gen::Launch& L, bool slab) const
 {
-    // Enough CTAs for every SM a few times over; long enough chunks that the z halo is a small part of what is read.
+    // Several waves of CTAs (a short last wave wastes little), and chunks long enough that the z halo is a small part of
+    // what is read (2 RZ planes of every 32 RZ).
     const long long tiles = slab ? static_cast<long long>((nx_ + 127) / 128) * ((ny_ + L.ty - 1) / L.ty)
                                  : static_cast<long long>((nx_ + 31) / 32) * ((ny_ + 7) / 8);
-    const long long want = static_cast<long long>(sms_) * (slab ? 3 : 6);
+    const long long want = static_cast<long long>(sms_) * (slab ? 12 : 16);
     const long long chunks = std::max<long long>(1, (want + tiles - 1) / tiles);
     int zchunk = static_cast<int>((nz_ + chunks - 1) / chunks);
-    if (L.rz > 0) zchunk = std::max(zchunk, std::min(nz_, 16 * L.rz));
+    if (L.rz > 0) zchunk = std::max(zchunk, std::min(nz_, 32 * L.rz));
     return std::max(1, zchunk);
 }
 
