@@ -172,6 +172,7 @@ __device__ __forceinline__ unsigned fe_warp_max(unsigned v)
 // keys once per block.
 struct FeAcc {
     double before, before_abs, after, after_abs;
+    float pb, pba, pa;  // this plane's fp32 partials of before, |before| and after (fe_acc_flush moves them to FP64)
     float lo, hi;
     unsigned bad, nan, first, changed;
 };
@@ -179,8 +180,19 @@ struct FeAcc {
 __device__ __forceinline__ void fe_acc_init(FeAcc& a)
 {
     a.before = 0.0; a.before_abs = 0.0; a.after = 0.0; a.after_abs = 0.0;
+    a.pb = 0.f; a.pba = 0.f; a.pa = 0.f;
     a.lo = __int_as_float(0x7f800000); a.hi = __int_as_float(0xff800000);
     a.bad = 0u; a.nan = 0u; a.first = 0u; a.changed = 0u;
+}
+
+// The lane's fp32 partials of one plane (its R rows of 4 cells: a few cells, rounded a few 1e-8 of their sum) into
+// the FP64 totals. Called once a plane, in a fixed order.
+__device__ __forceinline__ void fe_acc_flush(FeAcc& a)
+{
+    a.before += static_cast<double>(a.pb);
+    a.before_abs += static_cast<double>(a.pba);
+    a.after += static_cast<double>(a.pa);
+    a.pb = 0.f; a.pba = 0.f; a.pa = 0.f;
 }
 
 __device__ __forceinline__ void fe_acc_bad(FeAcc& a, float after, unsigned index)
@@ -198,12 +210,12 @@ __device__ __forceinline__ void fe_acc_row4(FeAcc& a, const float* before, const
     unsigned index0, bool totals_before, bool totals_after, bool range = true)
 {
     if (totals_before) {
-        a.before += static_cast<double>((before[0] + before[1]) + (before[2] + before[3]));
-        a.before_abs += static_cast<double>((fabsf(before[0]) + fabsf(before[1])) + (fabsf(before[2]) + fabsf(before[3])));
+        a.pb += (before[0] + before[1]) + (before[2] + before[3]);
+        a.pba += (fabsf(before[0]) + fabsf(before[1])) + (fabsf(before[2]) + fabsf(before[3]));
     }
     const float s4 = (after[0] + after[1]) + (after[2] + after[3]);
     if (totals_after) {
-        a.after += static_cast<double>(s4);
+        a.pa += s4;
     }
     if (range) {
         // The group's least and most (NaN ignored) give the bounds and the range test at once; a NaN or an infinity
@@ -249,6 +261,7 @@ __device__ __forceinline__ void fe_acc_cell(FeAcc& a, float before, float after,
 // straight into the record. `scratch` holds 4 doubles per warp. Every thread of the block calls it.
 __device__ __forceinline__ void fe_acc_block(FeAcc& a, double* scratch, double* partial, FeCheck* rec)
 {
+    fe_acc_flush(a);
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int warps = (blockDim.x + 31) >> 5;
@@ -536,6 +549,8 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
                 }
             }
         }
+#pragma unroll
+        for (int j = 0; j < P::NOUT; ++j) fe_acc_flush(acc[j]);
         if (z + 1 < ze) wait_upto(min(z + 1 + P::RZ, P::NZ - 1) - zlo);
         __syncthreads();
         const int release = z - P::RZ - zlo;

@@ -165,6 +165,7 @@ __global__ void __launch_bounds__(W * 32) heat7_tma(const __grid_constant__ FeTe
             }
             *reinterpret_cast<float4*>(a.out + at) = make_float4(o[0], o[1], o[2], o[3]);
         }
+        fe_acc_flush(acc);
         if (z + 1 < ze) {
             wait_upto(min(z + 2, nz - 1) - zlo);
         }
