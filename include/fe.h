@@ -188,6 +188,38 @@ int fe_law_stream(const fe_law* law, void** stream);
 /* Device time of `launches` back-to-back launches of term `term`'s fused gather pass (the roofline's kernel). */
 int fe_law_time_gather(fe_law* law, int term, int launches, float* ms);
 
+/* ---- batched Heston ADI: many options on uneven grids in one persistent launch -----------------------------------------
+ * The reference prices a batch as the z-planes of one lattice, every option on the same grid (bench/finance.py:253-288,
+ * bench/laws/heston_adi.law); here every option has its own grid and all are stepped by one persistent kernel (a CTA an
+ * option at a time, largest first), with the law's discretisation (tests/laws/heston_douglas.law, heston_hv.law) and
+ * tridiagonal solves by warp segments (a PCR/Thomas hybrid). x = ln S on [ln K - 3, ln K + 3] with h = 6 / nx; the
+ * variance rows var_j = sigma (j + 1/2) h; the put payoff averaged over each cell; price at (ln spot, v0) by bilinear
+ * interpolation between cell centres. */
+#define FE_ADI_DOUGLAS 0
+#define FE_ADI_HV 1
+typedef struct fe_heston_option {
+    int nx, ny;           /* powers of two: nx in [4, 512], ny in [4, 256] */
+    float strike, maturity, spot, v0;
+    float kappa, theta, sigma, rho, r;
+} fe_heston_option;
+typedef struct fe_heston_batch fe_heston_batch;
+/* n in [1, 65535] options, `steps` time steps each to its maturity, scheme FE_ADI_DOUGLAS or FE_ADI_HV. */
+int fe_heston_batch_create(const fe_heston_option* options, int n, int steps, int scheme, fe_heston_batch** out);
+void fe_heston_batch_destroy(fe_heston_batch* batch);
+/* Cells a lane holds along x and along y in the tridiagonal solves (4, 8 or 16 each); a line takes n / m lanes of a
+ * warp, which must be at most 32 for every option in the batch. */
+int fe_heston_batch_set_split(fe_heston_batch* batch, int mx, int my);
+/* Times short runs of every split that fits the batch and keeps the fastest (mx, my may be NULL). */
+int fe_heston_batch_autotune(fe_heston_batch* batch, int* mx, int* my);
+/* Sets up the payoffs and steps every option to maturity (asynchronous on the batch's stream). With use_graph the
+ * launch sequence is captured once into a CUDA graph and replayed. */
+int fe_heston_batch_run(fe_heston_batch* batch, int use_graph);
+/* Device time of one run (ms). */
+int fe_heston_batch_time(fe_heston_batch* batch, int use_graph, float* ms);
+/* The prices of the last run (n floats) and one option's grid (nx * ny floats, x fastest). Both wait for the run. */
+int fe_heston_batch_prices(fe_heston_batch* batch, float* host_prices);
+int fe_heston_batch_grid(fe_heston_batch* batch, int option, float* host_grid);
+
 #ifdef __cplusplus
 }
 #endif

@@ -62,6 +62,14 @@ class fe_violation(ctypes.Structure):
     ]
 
 
+class fe_heston_option(ctypes.Structure):
+    """Mirror of ``fe_heston_option`` (include/fe.h)."""
+
+    _fields_ = [("nx", _c.c_int), ("ny", _c.c_int), ("strike", _c.c_float), ("maturity", _c.c_float),
+                ("spot", _c.c_float), ("v0", _c.c_float), ("kappa", _c.c_float), ("theta", _c.c_float),
+                ("sigma", _c.c_float), ("rho", _c.c_float), ("r", _c.c_float)]
+
+
 class fe_step_info(ctypes.Structure):
     _fields_ = [("violations", _c.c_int), ("launches", _c.c_int), ("gpu_ms", _c.c_double)]
 
@@ -73,6 +81,7 @@ class fe_field_info(ctypes.Structure):
 
 FE_RANGE, FE_NOT_FINITE, FE_CONSERVATION, FE_SUBSTEP_CAP = 0, 1, 2, 3
 FE_STEP_IGNORE_MAX_DT = 1
+FE_ADI_DOUGLAS, FE_ADI_HV = 0, 1
 
 _p = _c.c_void_p
 _s = _c.c_size_t
@@ -129,6 +138,14 @@ SIGNATURES = {
     "fe_law_digest": (_i, [_p, _c.POINTER(_c.c_uint64)]),
     "fe_law_stream": (_i, [_p, _c.POINTER(_p)]),
     "fe_law_time_gather": (_i, [_p, _i, _i, _c.POINTER(_c.c_float)]),
+    "fe_heston_batch_create": (_i, [_c.POINTER(fe_heston_option), _i, _i, _i, _c.POINTER(_p)]),
+    "fe_heston_batch_destroy": (None, [_p]),
+    "fe_heston_batch_set_split": (_i, [_p, _i, _i]),
+    "fe_heston_batch_autotune": (_i, [_p, _c.POINTER(_i), _c.POINTER(_i)]),
+    "fe_heston_batch_run": (_i, [_p, _i]),
+    "fe_heston_batch_time": (_i, [_p, _i, _c.POINTER(_c.c_float)]),
+    "fe_heston_batch_prices": (_i, [_p, _p]),
+    "fe_heston_batch_grid": (_i, [_p, _i, _p]),
 }
 
 

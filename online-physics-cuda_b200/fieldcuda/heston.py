@@ -1,0 +1,104 @@
+"""Batched Heston ADI on the GPU (include/fe.h, fe_heston_batch_*): many European puts, each on its own grid, stepped
+to maturity by one persistent kernel.
+
+The reference prices a batch as the z-planes of one lattice, all options on one grid, through its law solver
+(bench/finance.py:253-288 with bench/laws/heston_adi.law). Here the options keep their own (nx, ny) and the whole
+batch is one launch sequence (payoffs, the persistent ADI kernel, the price read-out), optionally replayed as a CUDA
+graph. The discretisation is the law's: tests/laws/heston_douglas.law and heston_hv.law.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+DOUGLAS = _lib.FE_ADI_DOUGLAS
+HV = _lib.FE_ADI_HV
+
+FIELDS = ("nx", "ny", "strike", "maturity", "spot", "v0", "kappa", "theta", "sigma", "rho", "r")
+
+
+def option_array(options):
+    """A ctypes array of fe_heston_option from dicts (or objects with those attributes)."""
+    arr = (_lib.fe_heston_option * len(options))()
+    for i, o in enumerate(options):
+        for f in FIELDS:
+            setattr(arr[i], f, o[f] if isinstance(o, dict) else getattr(o, f))
+    return arr
+
+
+class HestonBatch:
+    """One batch of options: ``run`` prices them all, ``prices`` and ``grid`` read the results back."""
+
+    def __init__(self, options, steps, scheme=DOUGLAS):
+        self.options = list(options)
+        self.steps = int(steps)
+        self.scheme = scheme
+        self._arr = option_array(self.options)
+        handle = ctypes.c_void_p()
+        _lib.call("fe_heston_batch_create", self._arr, len(self.options), self.steps, scheme, ctypes.byref(handle))
+        self._h = handle
+
+    def close(self):
+        if self._h:
+            _lib.lib().fe_heston_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_split(self, mx, my):
+        """Cells a lane holds in the x and y tridiagonal solves (4, 8 or 16)."""
+        _lib.call("fe_heston_batch_set_split", self._h, mx, my)
+
+    def autotune(self):
+        """Times every split that fits and keeps the fastest; returns it as (mx, my)."""
+        mx, my = ctypes.c_int(), ctypes.c_int()
+        _lib.call("fe_heston_batch_autotune", self._h, ctypes.byref(mx), ctypes.byref(my))
+        return mx.value, my.value
+
+    def run(self, use_graph=False):
+        """Prices the batch (asynchronous on the batch's stream)."""
+        _lib.call("fe_heston_batch_run", self._h, int(bool(use_graph)))
+
+    def time(self, use_graph=True):
+        """Device time of one run, in ms."""
+        ms = ctypes.c_float()
+        _lib.call("fe_heston_batch_time", self._h, int(bool(use_graph)), ctypes.byref(ms))
+        return ms.value
+
+    def prices(self):
+        out = np.empty(len(self.options), np.float32)
+        _lib.call("fe_heston_batch_prices", self._h, out.ctypes.data_as(ctypes.c_void_p))
+        return out
+
+    def grid(self, i):
+        """Option i's grid after the last run, shape (ny, nx)."""
+        o = self._arr[i]
+        out = np.empty((o.ny, o.nx), np.float32)
+        _lib.call("fe_heston_batch_grid", self._h, i, out.ctypes.data_as(ctypes.c_void_p))
+        return out
+
+
+def sample_options(n, seed, sizes=((128, 64), (256, 128), (512, 256))):
+    """Seeded options with the batch benchmark's parameter ranges: strike U[80, 120], T U[0.25, 2], kappa U[0.5, 5],
+    theta U[0.01, 0.1], sigma U[0.1, 1], rho U[-0.9, -0.1], v0 U[0.01, 0.1], r U[0, 0.05], spot 100; grid sizes
+    drawn from ``sizes``."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        nx, ny = sizes[int(rng.integers(len(sizes)))]
+        out.append(dict(nx=nx, ny=ny, strike=float(rng.uniform(80, 120)), maturity=float(rng.uniform(0.25, 2.0)),
+                        spot=100.0, v0=float(rng.uniform(0.01, 0.1)), kappa=float(rng.uniform(0.5, 5)),
+                        theta=float(rng.uniform(0.01, 0.1)), sigma=float(rng.uniform(0.1, 1.0)),
+                        rho=float(rng.uniform(-0.9, -0.1)), r=float(rng.uniform(0.0, 0.05))))
+    return out

@@ -41,3 +41,24 @@ def test_key_to_float_roundtrip():
         b = np.array([v], dtype=np.float32).view(np.uint32)[0]
         key = (~b & 0xFFFFFFFF) if (b & 0x80000000) else (b | 0x80000000)
         assert np.float32(lib.fe_key_to_float(int(key))) == np.float32(v)
+
+
+def test_heston_batch_rejects_bad_options_before_touching_a_device():
+    import ctypes
+    from fieldcuda import _lib
+    from fieldcuda.heston import option_array, sample_options
+    lib = _lib.lib()
+    good = sample_options(3, 1)
+    for bad in (dict(nx=96), dict(ny=512), dict(strike=-1.0), dict(sigma=0.0), dict(maturity=0.0), dict(spot=0.0)):
+        opts = [dict(good[0]), dict(good[1], **bad), dict(good[2])]
+        h = ctypes.c_void_p()
+        assert lib.fe_heston_batch_create(option_array(opts), 3, 8, 0, ctypes.byref(h)) == _lib.FE_EINVAL
+        assert "option 1" in _lib.last_error()
+        assert not h.value
+    h = ctypes.c_void_p()
+    assert lib.fe_heston_batch_create(option_array(good), 3, 8, 2, ctypes.byref(h)) == _lib.FE_EINVAL
+    status = lib.fe_heston_batch_create(option_array(good), 3, 8, 0, ctypes.byref(h))
+    if status == _lib.FE_OK:
+        lib.fe_heston_batch_destroy(h)
+    else:
+        assert status == _lib.FE_ENODEV
