@@ -247,6 +247,105 @@ def copy_roof_gbs(cells, stream, reps=10):
     return 2 * 4 * cells * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9
 
 
+HESTON_EXPLICIT_LAW = os.path.join(ROOT, "tests", "laws", "heston_explicit.law")
+HESTON_CF = os.path.join(ROOT, "tests", "golden", "heston", "cf_2048.npz")
+HESTON_BUCKETS = ((128, 64), (256, 128), (512, 256))
+
+
+def heston_batch_section(stream_sync):
+    """Batched Heston ADI (Douglas, theta = 1/2): 2048 seeded options on their own grids (128 x 64, 256 x 128 or 512 x
+    256), 512 steps, priced in one persistent launch (autotuned, CUDA-graph replayed), against the plain method at the
+    same grids: the explicit law (tests/laws/heston_explicit.law, the same operator, stepped at its stability limit)
+    through the law backend, the reference's way of batching (every bucket's options as the z-planes of one lattice).
+    Errors are against FP64 characteristic-function prices of the same options (tests/golden/heston/cf_2048.npz)."""
+    import numpy as np
+    import torch
+    from fieldcuda.heston import DOUGLAS, HestonBatch, lattice_fields, price_at, sample_options
+    from fieldcuda.solver import Solver
+
+    n, steps = 2048, 512
+    opts = sample_options(n, 1)
+    cf = None
+    if os.path.exists(HESTON_CF):
+        z = np.load(HESTON_CF)
+        if int(z["seed"]) == 1 and len(z["price"]) == n and np.allclose(z["strike"], [o["strike"] for o in opts]):
+            cf = z["price"]
+    with HestonBatch(opts, steps, DOUGLAS) as b:
+        split = b.autotune()
+        clusters, tasks = b.layout()
+        b.run(use_graph=True)
+        prices = b.prices().astype(np.float64)
+        runs = [b.time(use_graph=True) for _ in range(3)]
+    ms = statistics.median(runs)
+    cells = sum(o["nx"] * o["ny"] for o in opts)
+    out = {"options": n, "steps": steps, "scheme": "Douglas (theta = 1/2)", "ms": ms, "options_per_s": n / (ms * 1e-3),
+           "cell_steps_per_s": cells * steps / (ms * 1e-3), "split": {"mx": split[0], "sy": split[1], "threads": split[2]},
+           "clusters": clusters, "tasks": tasks,
+           "hbm_bytes": 8 * cells, "hbm_note": "each option's state stays in shared memory for all its steps: 8 B a cell a run"}
+    if cf is not None:
+        err = np.abs(prices - cf)
+        out["error_vs_cf"] = {"median": float(np.median(err)), "p90": float(np.percentile(err, 90)), "max": float(err.max())}
+
+    # The plain method: explicit Euler on each bucket's lattice at its stability limit. Its cost is measured per
+    # substep on up to 128 planes of the bucket and scaled by planes and by the substeps that reach each bucket's
+    # longest maturity (the explicit pass streams the lattice from HBM, so its time grows with the planes).
+    law = open(HESTON_EXPLICIT_LAW).read()
+    plain_ms = 0.0
+    plain = {}
+    sample_err = {"adi": [], "plain": []}
+    for nx, ny in HESTON_BUCKETS:
+        group = [i for i, o in enumerate(opts) if (o["nx"], o["ny"]) == (nx, ny)]
+        if not group:
+            continue
+        planes = [opts[i] for i in group[:128]]
+        fields, h = lattice_fields(planes, nx, ny)
+        s = Solver(law, nx, ny, len(planes), h, "heston_explicit.law")
+        for k, v in fields.items():
+            s.set_field(k, v)
+        max_dt = 0.25 * h / (max(o["sigma"] for o in planes) * ny)   # the law's limit: 0.25 h^2 / (sig_v h ny)
+        sub = 64
+        s.step(sub * max_dt * 0.999)
+        st = torch.cuda.ExternalStream(s.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stream_sync()
+        e0.record(st)
+        s.step(sub * max_dt * 0.999)
+        e1.record(st)
+        st.synchronize()
+        per_sub = e0.elapsed_time(e1) / max(1, max(s.last_substeps()))
+        s.close()
+        t_max = max(opts[i]["maturity"] for i in group)
+        sig_max = max(opts[i]["sigma"] for i in group)
+        subs = int(np.ceil(t_max / (0.25 * h / (sig_max * ny))))
+        bucket_ms = per_sub * (len(group) / len(planes)) * subs
+        plain_ms += bucket_ms
+        plain[f"{nx}x{ny}"] = {"options": len(group), "substeps": subs, "ms_per_substep_128_planes": per_sub, "ms": bucket_ms}
+        # Equal error: two options of the bucket priced by the plain method to maturity (each alone), beside the batch.
+        if cf is not None:
+            for i in group[:2]:
+                o = opts[i]
+                f1, _ = lattice_fields([o], nx, ny)
+                s1 = Solver(law, nx, ny, 1, h, "heston_explicit.law")
+                for k, v in f1.items():
+                    s1.set_field(k, v)
+                lim = 0.25 * h / (o["sigma"] * ny)
+                nsteps = int(np.ceil(o["maturity"] / (4000 * lim)))
+                for _ in range(nsteps):
+                    s1.step(o["maturity"] / nsteps)
+                p = price_at(s1.values("V")[0], o)
+                s1.close()
+                sample_err["plain"].append(abs(p - cf[i]))
+                sample_err["adi"].append(float(abs(prices[i] - cf[i])))
+    out["plain"] = {"method": "explicit Euler law (tests/laws/heston_explicit.law) through fe_law_step, same grids",
+                    "ms": plain_ms, "options_per_s": n / (plain_ms * 1e-3), "buckets": plain}
+    if sample_err["plain"]:
+        out["equal_error_sample"] = {"options": len(sample_err["plain"]),
+                                     "adi_abs_err": [round(v, 6) for v in sample_err["adi"]],
+                                     "plain_abs_err": [round(v, 6) for v in sample_err["plain"]]}
+    out["speedup_vs_plain"] = plain_ms / ms
+    return out
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -338,6 +437,10 @@ def run_ours(args, world, rank, local):
             cpu = {"value": BYTES_PER_CELL * cells / (ms * 1e-3) / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
                    "sample": f"1 step of the {n}^3 heat law, numpy restatement (oracle/heat.py)"}
 
+    heston = None
+    if not args.no_heston:
+        heston = heston_batch_section(torch.cuda.synchronize)
+
     if rank != 0:
         return
     print(json.dumps({
@@ -361,6 +464,7 @@ def run_ours(args, world, rank, local):
                         "fe_law_fetch of the state to pinned host memory (wall clock)"},
         "gpu_launches": launches,
         "clocks": clk,
+        "heston_batch": heston,
     }))
 
 
@@ -372,6 +476,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-heston", action="store_true", help="skip the batched Heston ADI section")
     args = ap.parse_args()
     world, rank, local = init_dist()
     try:

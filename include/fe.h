@@ -190,11 +190,13 @@ int fe_law_time_gather(fe_law* law, int term, int launches, float* ms);
 
 /* ---- batched Heston ADI: many options on uneven grids in one persistent launch -----------------------------------------
  * The reference prices a batch as the z-planes of one lattice, every option on the same grid (bench/finance.py:253-288,
- * bench/laws/heston_adi.law); here every option has its own grid and all are stepped by one persistent kernel (a CTA an
- * option at a time, largest first), with the law's discretisation (tests/laws/heston_douglas.law, heston_hv.law) and
- * tridiagonal solves by warp segments (a PCR/Thomas hybrid). x = ln S on [ln K - 3, ln K + 3] with h = 6 / nx; the
- * variance rows var_j = sigma (j + 1/2) h; the put payoff averaged over each cell; price at (ln spot, v0) by bilinear
- * interpolation between cell centres. */
+ * bench/laws/heston_adi.law); here every option has its own grid and all are stepped by one persistent kernel of 8-CTA
+ * clusters that keeps each option's state in shared memory from its first step to its last (an option of more than 16K
+ * cells split by rows over 2, 4 or 8 CTAs of a cluster, neighbours read over distributed shared memory), with the law's
+ * discretisation (tests/laws/heston_douglas.law, heston_hv.law): x lines by warp segments (PCR/Thomas hybrid), y lines
+ * by the partition method across the CTAs. x = ln S on [ln K - 3, ln K + 3] with h = 6 / nx; the variance rows var_j =
+ * sigma (j + 1/2) h; the put payoff averaged over each cell; price at (ln spot, v0) by bilinear interpolation between
+ * cell centres. No counterpart in the reference's C++ API. */
 #define FE_ADI_DOUGLAS 0
 #define FE_ADI_HV 1
 typedef struct fe_heston_option {
@@ -206,11 +208,14 @@ typedef struct fe_heston_batch fe_heston_batch;
 /* n in [1, 65535] options, `steps` time steps each to its maturity, scheme FE_ADI_DOUGLAS or FE_ADI_HV. */
 int fe_heston_batch_create(const fe_heston_option* options, int n, int steps, int scheme, fe_heston_batch** out);
 void fe_heston_batch_destroy(fe_heston_batch* batch);
-/* Cells a lane holds along x and along y in the tridiagonal solves (4, 8 or 16 each); a line takes n / m lanes of a
- * warp, which must be at most 32 for every option in the batch. */
-int fe_heston_batch_set_split(fe_heston_batch* batch, int mx, int my);
-/* Times short runs of every split that fits the batch and keeps the fastest (mx, my may be NULL). */
-int fe_heston_batch_autotune(fe_heston_batch* batch, int* mx, int* my);
+/* The split of the work: mx cells a lane holds in the x solves (4, 8 or 16; an x line takes nx / mx lanes of a warp,
+ * at most 32 for every option), sy the most row blocks a CTA cuts a column into for the y solves (1, 2, 4, 8 or 16),
+ * threads a CTA (256, 384 or 512: fewer threads, more registers each). */
+int fe_heston_batch_set_split(fe_heston_batch* batch, int mx, int sy, int threads);
+/* Times short runs of every split that fits the batch and keeps the fastest (the outputs may be NULL). */
+int fe_heston_batch_autotune(fe_heston_batch* batch, int* mx, int* sy, int* threads);
+/* The persistent grid's 8-CTA clusters and the batch's tasks (8 / C options split over C CTAs each). */
+int fe_heston_batch_layout(const fe_heston_batch* batch, int* clusters, int* tasks);
 /* Sets up the payoffs and steps every option to maturity (asynchronous on the batch's stream). With use_graph the
  * launch sequence is captured once into a CUDA graph and replayed. */
 int fe_heston_batch_run(fe_heston_batch* batch, int use_graph);

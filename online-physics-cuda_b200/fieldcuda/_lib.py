@@ -140,8 +140,9 @@ SIGNATURES = {
     "fe_law_time_gather": (_i, [_p, _i, _i, _c.POINTER(_c.c_float)]),
     "fe_heston_batch_create": (_i, [_c.POINTER(fe_heston_option), _i, _i, _i, _c.POINTER(_p)]),
     "fe_heston_batch_destroy": (None, [_p]),
-    "fe_heston_batch_set_split": (_i, [_p, _i, _i]),
-    "fe_heston_batch_autotune": (_i, [_p, _c.POINTER(_i), _c.POINTER(_i)]),
+    "fe_heston_batch_set_split": (_i, [_p, _i, _i, _i]),
+    "fe_heston_batch_autotune": (_i, [_p, _c.POINTER(_i), _c.POINTER(_i), _c.POINTER(_i)]),
+    "fe_heston_batch_layout": (_i, [_p, _c.POINTER(_i), _c.POINTER(_i)]),
     "fe_heston_batch_run": (_i, [_p, _i]),
     "fe_heston_batch_time": (_i, [_p, _i, _c.POINTER(_c.c_float)]),
     "fe_heston_batch_prices": (_i, [_p, _p]),

@@ -3,8 +3,9 @@ to maturity by one persistent kernel.
 
 The reference prices a batch as the z-planes of one lattice, all options on one grid, through its law solver
 (bench/finance.py:253-288 with bench/laws/heston_adi.law). Here the options keep their own (nx, ny) and the whole
-batch is one launch sequence (payoffs, the persistent ADI kernel, the price read-out), optionally replayed as a CUDA
-graph. The discretisation is the law's: tests/laws/heston_douglas.law and heston_hv.law.
+batch is one launch sequence (payoffs, the persistent ADI kernel of 8-CTA clusters that holds every option's state in
+shared memory from its first step to its last, the price read-out), optionally replayed as a CUDA graph. The
+discretisation is the law's: tests/laws/heston_douglas.law and heston_hv.law.
 """
 import ctypes
 
@@ -56,15 +57,22 @@ class HestonBatch:
         except Exception:
             pass
 
-    def set_split(self, mx, my):
-        """Cells a lane holds in the x and y tridiagonal solves (4, 8 or 16)."""
-        _lib.call("fe_heston_batch_set_split", self._h, mx, my)
+    def set_split(self, mx, sy, threads=384):
+        """Cells a lane holds in the x solves (4, 8 or 16), the most row blocks a CTA cuts a column into for the y
+        solves (1 .. 16), and threads a CTA (256, 384 or 512)."""
+        _lib.call("fe_heston_batch_set_split", self._h, mx, sy, threads)
 
     def autotune(self):
-        """Times every split that fits and keeps the fastest; returns it as (mx, my)."""
-        mx, my = ctypes.c_int(), ctypes.c_int()
-        _lib.call("fe_heston_batch_autotune", self._h, ctypes.byref(mx), ctypes.byref(my))
-        return mx.value, my.value
+        """Times every split that fits and keeps the fastest; returns it as (mx, sy, threads)."""
+        mx, sy, nt = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.call("fe_heston_batch_autotune", self._h, ctypes.byref(mx), ctypes.byref(sy), ctypes.byref(nt))
+        return mx.value, sy.value, nt.value
+
+    def layout(self):
+        """(clusters of the persistent grid, tasks of the batch)."""
+        c, t = ctypes.c_int(), ctypes.c_int()
+        _lib.call("fe_heston_batch_layout", self._h, ctypes.byref(c), ctypes.byref(t))
+        return c.value, t.value
 
     def run(self, use_graph=False):
         """Prices the batch (asynchronous on the batch's stream)."""
@@ -102,3 +110,46 @@ def sample_options(n, seed, sizes=((128, 64), (256, 128), (512, 256))):
                         theta=float(rng.uniform(0.01, 0.1)), sigma=float(rng.uniform(0.1, 1.0)),
                         rho=float(rng.uniform(-0.9, -0.1)), r=float(rng.uniform(0.0, 0.05))))
     return out
+
+
+def cell_payoff(strike, nx):
+    """The put payoff averaged over each of nx cells of x = ln S on [ln K - 3, ln K + 3] (FP64, stored as float)."""
+    h = 6.0 / nx
+    lk = np.log(strike)
+    x = lk - 3.0 + (np.arange(nx) + 0.5) * h
+    lo = x - 0.5 * h
+    hi = np.minimum(x + 0.5 * h, lk)
+    v = np.where(hi > lo, (strike * (hi - lo) - (np.exp(hi) - np.exp(lo))) / h, 0.0)
+    return v.astype(np.float32)
+
+
+def lattice_fields(options, nx, ny):
+    """The fields of the Heston laws (tests/laws/heston_*.law) for options of one grid size as the z-planes of one
+    lattice, the reference's way of batching (bench/finance.py:253-267): V the cell-averaged payoff, var the rows'
+    variances sigma (j + 1/2) h, the model numbers as per-plane constants. Returns (fields, h)."""
+    nz = len(options)
+    h = 6.0 / nx
+    f32 = np.float32
+    shape = (nz, ny, nx)
+    out = {k: np.empty(shape, f32) for k in ("V", "var", "kappa", "theta", "sig_v", "rho", "r")}
+    for z, o in enumerate(options):
+        out["V"][z] = cell_payoff(o["strike"], nx)[None, :]
+        out["var"][z] = (o["sigma"] * (np.arange(ny) + 0.5) * h).astype(f32)[:, None]
+        for k, name in (("kappa", "kappa"), ("theta", "theta"), ("sig_v", "sigma"), ("rho", "rho"), ("r", "r")):
+            out[k][z] = f32(o[name])
+    return out, h
+
+
+def price_at(grid, option):
+    """Bilinear price at (ln spot, v0) between the cell centres of one option's (ny, nx) grid, as the batch's read-out."""
+    ny, nx = grid.shape
+    h = 6.0 / nx
+    x0 = np.log(option["strike"]) - 3.0 + 0.5 * h
+    fx = (np.log(option["spot"]) - x0) / h
+    fy = option["v0"] / (option["sigma"] * h) - 0.5
+    i0 = int(max(0, min(nx - 2, np.floor(fx))))
+    j0 = int(max(0, min(ny - 2, np.floor(fy))))
+    tx = min(max(fx - i0, 0.0), 1.0)
+    ty = min(max(fy - j0, 0.0), 1.0)
+    g = grid.astype(np.float64)
+    return float((1 - ty) * ((1 - tx) * g[j0, i0] + tx * g[j0, i0 + 1]) + ty * ((1 - tx) * g[j0 + 1, i0] + tx * g[j0 + 1, i0 + 1]))

@@ -86,6 +86,7 @@ def cases():
     f, h = heston_fields(32, 16, 3, 7)
     out.append(dict(name="heston_douglas", law="heston_douglas.law", shape=(3, 16, 32), h=h, dt=0.01, steps=4, fields=f))
     out.append(dict(name="heston_hv", law="heston_hv.law", shape=(3, 16, 32), h=h, dt=0.01, steps=4, fields=f))
+    out.append(dict(name="heston_explicit", law="heston_explicit.law", shape=(3, 16, 32), h=h, dt=0.01, steps=3, fields=f))
     return out
 
 

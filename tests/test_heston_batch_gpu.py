@@ -52,7 +52,7 @@ def small_options(seed):
 
 
 @pytest.mark.parametrize("scheme,law_name", [(0, "heston_douglas"), (1, "heston_hv")])
-@pytest.mark.parametrize("split", [(16, 8), (4, 4)])
+@pytest.mark.parametrize("split", [(16, 4, 384), (4, 1, 512), (8, 16, 256)])
 def test_batch_matches_the_law_oracle(cuda, scheme, law_name, split):
     from fieldcuda.heston import HestonBatch
     opts = small_options(3)
@@ -67,6 +67,27 @@ def test_batch_matches_the_law_oracle(cuda, scheme, law_name, split):
             want = oracle_grid(o, steps, law_name).astype(np.float64)
             rel = np.abs(got - want).max() / np.abs(want).max()
             assert rel <= ORACLE_TOL, f"option {i} ({o['nx']}x{o['ny']}): relative difference {rel:.3g}"
+
+
+@pytest.mark.parametrize("scheme,law_name", [(0, "heston_douglas"), (1, "heston_hv")])
+def test_options_split_over_several_ctas_match_the_law_oracle(cuda, scheme, law_name):
+    """Options of more than 16K cells or 128 rows are split by rows over 2, 4 or 8 CTAs of a cluster: the rows above and
+    below a CTA's block come from its neighbours' shared memory and the y lines are solved across the CTAs."""
+    from fieldcuda.heston import HestonBatch, sample_options
+    sizes = ((256, 128), (512, 256), (64, 256), (512, 64), (128, 256), (32, 16))
+    opts = sample_options(len(sizes), 11, sizes=sizes)
+    for o, (nx, ny) in zip(opts, sizes):
+        o["nx"], o["ny"] = nx, ny
+    steps = 10
+    with HestonBatch(opts, steps, scheme) as b:
+        for split in ((16, 1, 512), (16, 16, 256), (16, 4, 384)):
+            b.set_split(*split)
+            b.run(use_graph=True)
+            for i, o in enumerate(opts):
+                got = b.grid(i).astype(np.float64)
+                want = oracle_grid(o, steps, law_name).astype(np.float64)
+                rel = np.abs(got - want).max() / np.abs(want).max()
+                assert rel <= ORACLE_TOL, f"split {split} option {i} ({o['nx']}x{o['ny']}): relative difference {rel:.3g}"
 
 
 def test_graph_replay_and_schedule_do_not_change_results(cuda):
@@ -90,17 +111,19 @@ def test_splits_agree_and_autotune_picks_one_that_fits(cuda):
     from fieldcuda.heston import HestonBatch, sample_options
     opts = sample_options(24, 9, sizes=((64, 32), (128, 64)))
     with HestonBatch(opts, 24, 1) as b:
-        b.set_split(16, 16)
+        b.set_split(16, 16, 512)
         b.run()
         ref = b.prices().astype(np.float64)
-        mx, my = b.autotune()
-        assert mx in (4, 8, 16) and my in (4, 8, 16)
-        assert 128 // mx <= 32 and 64 // my <= 32
+        mx, sy, nt = b.autotune()
+        assert mx in (4, 8, 16) and sy in (1, 2, 4, 8, 16) and nt in (256, 384, 512)
+        assert 128 // mx <= 32
         b.run(use_graph=True)
         got = b.prices().astype(np.float64)
         assert np.abs(got - ref).max() <= 1e-4 * np.abs(ref).max()
         with pytest.raises(Exception):
-            b.set_split(2, 8)
+            b.set_split(2, 8, 384)
+        with pytest.raises(Exception):
+            b.set_split(16, 8, 320)
 
 
 def cf_price(o):
