@@ -346,6 +346,90 @@ def heston_batch_section(stream_sync):
     return out
 
 
+def multifield_section(n, steps, warmup, stream_sync):
+    """The 43-term, 6-field generated law (tests/laws/multifield43.law) at n^3 through the law backend: median step
+    time and effective bandwidth at its algorithmic bytes (every term reads and writes its fields once)."""
+    import numpy as np
+    import torch
+    from fieldcuda.solver import Solver
+    from fieldcuda.workloads import multifield_bytes_per_cell, multifield_law
+
+    text, rw = multifield_law(0)
+    h = 1.0 / n
+    dt = 0.1 * h * h
+    s = Solver(text, n, n, n, h, "multifield43.law")
+    rng = np.random.default_rng(43)
+    for i in range(6):
+        s.set_field(f"f{i}", rng.uniform(-1, 1, (n, n, n)).astype(np.float32))
+    s.set_deferred(True)
+    for _ in range(warmup):
+        s.step(dt)
+    s.sync()
+    st = torch.cuda.ExternalStream(s.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream_sync()
+    e0.record(st)
+    launches = 0
+    for _ in range(steps):
+        s.step(dt)
+        launches += s.profile()["launches"]
+    e1.record(st)
+    st.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    s.sync()
+    broken = s.violations()
+    substeps = sum(s.last_substeps())
+    s.close()
+    bpc = multifield_bytes_per_cell(rw)
+    return {"law": "43 terms, 6 fp32 fields (tests/laws/multifield43.law, seed 0)", "cells": n ** 3, "dt": dt,
+            "ms_per_step": ms, "term_passes_per_step": substeps, "launches_per_step": launches / steps,
+            "algorithmic_bytes_per_cell_step": bpc, "effective_gbs": bpc * n ** 3 / (ms * 1e-3) / 1e9,
+            "violations": len(broken)}
+
+
+HESTON_DOUGLAS_LAW = os.path.join(ROOT, "tests", "laws", "heston_douglas.law")
+HESTON_CALIB = os.path.join(ROOT, "tests", "golden", "heston", "calib_512.npz")
+
+
+def calibration_section():
+    """The adjoint calibration: loss = sum (price - target)^2 over 512 options (one maturity, strikes U[80, 120]) on one
+    256 x 128 lattice (the options as its z-planes), 512 Douglas ADI steps, and its gradient with respect to (kappa,
+    theta, sigma, rho, v0) by the IR-generated adjoint law with sqrt(N) checkpoints behind torch.autograd; checked
+    against central differences (eps = 1e-3 relative) of the same FP32 loss. Targets: FP64 characteristic-function
+    prices under a seeded ground truth plus N(0, 1e-4) noise (tests/golden/heston/calib_512.npz)."""
+    import numpy as np
+    from fieldcuda.heston import Calibration, calibration_options
+
+    z = np.load(HESTON_CALIB)
+    strikes, common, truth = calibration_options(512, int(z["seed"]))
+    nx, ny, steps = 256, 128, 512
+    cal = Calibration(open(HESTON_DOUGLAS_LAW).read(), strikes, common["maturity"], common["spot"], common["r"],
+                      z["targets"], nx, ny, steps)
+    x = np.array([truth["kappa"] * 1.3, truth["theta"] * 0.8, truth["sigma"] * 1.1, truth["rho"] * 0.9, truth["v0"] * 1.2])
+    cal.loss_and_grad(x)
+    t0 = time.perf_counter()
+    loss, grad = cal.loss_and_grad(x)
+    ms_grad = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    cal.loss_only(x)
+    ms_fwd = (time.perf_counter() - t0) * 1e3
+    fd = []
+    for i in range(5):
+        e = 1e-3 * abs(x[i])
+        xp, xm = x.copy(), x.copy()
+        xp[i] += e
+        xm[i] -= e
+        fd.append((cal.loss_only(xp) - cal.loss_only(xm)) / (2 * e))
+    cal.close()
+    fd = np.array(fd)
+    return {"options": 512, "lattice": f"{nx} x {ny} x 512 planes", "steps": steps,
+            "checkpoints": int(np.ceil(np.sqrt(steps))), "loss": loss,
+            "gradient": dict(zip(Calibration.NAMES, map(float, grad))), "central_fd": dict(zip(Calibration.NAMES, map(float, fd))),
+            "fd_rel_err": dict(zip(Calibration.NAMES, map(float, np.abs(grad - fd) / np.maximum(np.abs(fd), 1e-12)))),
+            "ms_loss_and_gradient": ms_grad, "ms_loss": ms_fwd,
+            "what": "wall clock of one loss + gradient (forward, checkpointed recompute, adjoint law backward)"}
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -440,6 +524,12 @@ def run_ours(args, world, rank, local):
     heston = None
     if not args.no_heston:
         heston = heston_batch_section(torch.cuda.synchronize)
+    multifield = None
+    if not args.no_multifield:
+        multifield = multifield_section(256, 10, 3, torch.cuda.synchronize)
+    calibration = None
+    if not args.no_calibration:
+        calibration = calibration_section()
 
     if rank != 0:
         return
@@ -465,6 +555,8 @@ def run_ours(args, world, rank, local):
         "gpu_launches": launches,
         "clocks": clk,
         "heston_batch": heston,
+        "multifield_256": multifield,
+        "adjoint_calibration": calibration,
     }))
 
 
@@ -477,6 +569,8 @@ def main():
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-heston", action="store_true", help="skip the batched Heston ADI section")
+    ap.add_argument("--no-multifield", action="store_true", help="skip the 43-term multi-field law section")
+    ap.add_argument("--no-calibration", action="store_true", help="skip the adjoint calibration section")
     args = ap.parse_args()
     world, rank, local = init_dist()
     try:

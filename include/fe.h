@@ -140,6 +140,11 @@ void fe_law_destroy(fe_law* law);
  * on the generated source (no GPU needed). */
 int fe_law_ir_json(const char* law_text, char* buf, size_t cap, size_t* needed);
 int fe_law_ir_listing(const char* law_text, char* buf, size_t cap, size_t* needed);
+/* The adjoint law of `term` (NULL or "": the first), as law text: reverse mode over the term's SSA instructions, the
+ * primal fields as static inputs, X__adj the cotangent of field or param X, tridiagonal solves by their transposes
+ * (replaces src/field/ir/Adjoint.hpp:24 adjoint_law, which refuses tridiag). FE_EUNSUP with the reason for ops that
+ * have no adjoint here. */
+int fe_law_adjoint(const char* law_text, const char* term, char* buf, size_t cap, size_t* needed);
 int fe_law_source(const char* law_text, int nx, int ny, int nz, double h, char* buf, size_t cap, size_t* needed);
 int fe_law_compile_check(const char* law_text, int nx, int ny, int nz, double h);
 

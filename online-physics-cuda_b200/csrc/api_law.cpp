@@ -1,6 +1,7 @@
 // C-ABI of the law backend (include/fe.h, "the law backend").
 #include "../../include/fe.h"
 
+#include "adjoint.hpp"
 #include "api_common.hpp"
 #include "engine.hpp"
 
@@ -98,6 +99,16 @@ int fe_law_ir_listing(const char* law_text, char* buf, size_t cap, size_t* neede
     if (!compile_law(law_text, law, why)) return fe::fail(FE_ELAW, why);
     const fe::ir::Module m = fe::ir::lower(law);
     return put_text(fe::ir::describe(m, law), buf, cap, needed);
+}
+
+int fe_law_adjoint(const char* law_text, const char* term, char* buf, size_t cap, size_t* needed)
+{
+    fe::law::Law law;
+    std::string why;
+    if (!compile_law(law_text, law, why)) return fe::fail(FE_ELAW, why);
+    const std::string text = fe::adjoint::adjoint_law(law, term ? term : "", why);
+    if (text.empty()) return fe::fail(FE_EUNSUP, why);
+    return put_text(text, buf, cap, needed);
 }
 
 int fe_law_source(const char* law_text, int nx, int ny, int nz, double h, char* buf, size_t cap, size_t* needed)

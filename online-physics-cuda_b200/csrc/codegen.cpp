@@ -467,7 +467,7 @@ private:
             rz = std::max(rz, pb.reach[k].z);
         }
         L.rz = rz;
-        if ((nx_ % 4) != 0 || pb.sources.empty() || pb.sources.size() > FE_MAX_SRC_HOST) return false;
+        if ((nx_ % 4) != 0 || pb.sources.empty() || pb.sources.size() > FE_MAX_MAP_HOST) return false;
         for (const Source& s : pb.sources) {
             if (128 + 2 * s.ax > 256 || s.ry > 64) return false;
         }
@@ -535,7 +535,8 @@ private:
         return safe;
     }
 
-    static constexpr std::size_t FE_MAX_SRC_HOST = 12;
+    static constexpr std::size_t FE_MAX_SRC_HOST = 32;   // FE_MAX_SRC
+    static constexpr std::size_t FE_MAX_MAP_HOST = 12;   // FE_MAX_MAP: a slab pass stages at most this many sources
     static constexpr std::size_t FE_MAX_OUT_HOST = 8;
 
     // A pass: computes `outs` (stage bodies, or the gather's targets) at every cell.
@@ -570,7 +571,7 @@ private:
         emit_functions(f, pb, roots, bodies);
         if (pb.sources.size() > FE_MAX_SRC_HOST || outs.size() > FE_MAX_OUT_HOST) {
             why = "a pass of '" + tag + "' reads " + std::to_string(pb.sources.size()) + " buffers and writes " + std::to_string(outs.size()) +
-                " (at most 12 and 8)";
+                " (at most 32 and 8)";
             return false;
         }
         L.kind = Launch::Pass;
@@ -639,8 +640,10 @@ private:
         f << "namespace " << ns << " {\n";
         std::vector<int> roots(in.args.begin(), in.args.end());
         emit_functions(f, pb, roots, false);
-        L.kind = in.index == 0 ? Launch::TridiagX : Launch::TridiagYZ;
-        L.axis = in.index;
+        const int axis = in.index % 3;
+        const bool transposed = in.index >= 3;
+        L.kind = axis == 0 ? Launch::TridiagX : Launch::TridiagYZ;
+        L.axis = axis;
         L.sources = pb.sources;
         L.slab = false;
         L.ty = 16;
@@ -650,12 +653,30 @@ private:
         L.checked_fields = {-1, -1};
         emit_traits(f, pb, L, 2, {0, 0});
         f << "    template <class C> static __device__ __forceinline__ void coef(const C& c, int x, int y, int z, float& lo, float& di, float& up, float& rhs) {\n"
-          << "        constexpr bool IN = false;\n"
-          << "        lo = " << v(in.args[0]) << "; up = " << v(in.args[2]) << "; di = " << v(in.args[1]) << "; rhs = " << v(in.args[3]) << ";\n    }\n";
+          << "        constexpr bool IN = false;\n";
+        if (!transposed) {
+            f << "        lo = " << v(in.args[0]) << "; up = " << v(in.args[2]) << "; di = " << v(in.args[1]) << "; rhs = " << v(in.args[3]) << ";\n    }\n";
+        } else {
+            // The transpose of the edge-repeating matrix: below the diagonal the previous cell's `up`, above it the next
+            // cell's `lo`, the folded edge terms on the diagonal (so the pass's own folding adds zeros).
+            const char* q = axis == 0 ? "x" : (axis == 1 ? "y" : "z");
+            const char* n = axis == 0 ? "NX" : (axis == 1 ? "NY" : "NZ");
+            auto at = [&](int arg, int d) {
+                const std::string s = std::string(q) + (d < 0 ? " - 1" : " + 1");
+                return axis == 0 ? v(in.args[arg], s) : (axis == 1 ? v(in.args[arg], "x", s) : v(in.args[arg], "x", "y", s));
+            };
+            f << "        const float l0 = " << v(in.args[0]) << ", u0 = " << v(in.args[2]) << ";\n"
+              << "        lo = " << q << " > 0 ? " << at(2, -1) << " : 0.f;\n"
+              << "        up = " << q << " + 1 < P::" << n << " ? " << at(0, +1) << " : 0.f;\n"
+              << "        di = " << v(in.args[1]) << ";\n"
+              << "        if (" << q << " == 0) di += l0;\n"
+              << "        if (" << q << " + 1 == P::" << n << ") di += u0;\n"
+              << "        rhs = " << v(in.args[3]) << ";\n    }\n";
+        }
         f << "    template <bool IN, class C> static __device__ __forceinline__ void cell(const C&, int, int, int, float*, float*) {}\n";
         f << "};\n}\n";
         L.kernel = "fe_tri_" + tag;
-        if (in.index == 0) {
+        if (axis == 0) {
             if (nx_ > 640) {
                 why = "tridiag_x keeps a line in shared memory: nx up to 640";
                 return false;
@@ -665,7 +686,7 @@ private:
               << "::P>(a); }\n";
         } else {
             f << "extern \"C\" __global__ void __launch_bounds__(128) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_tridiag_yz_pass<"
-              << ns << "::P, " << in.index << ">(a); }\n";
+              << ns << "::P, " << axis << ">(a); }\n";
         }
         out_ << f.str();
         return true;

@@ -36,11 +36,13 @@ struct FeCheck {
 
 // The one parameter block of every generated pass kernel (a fused gather, or a group of stored stages): the host fills
 // it, the kernel reads it as a __grid_constant__. Sources are the buffers the pass reads (a field's current buffer or a
-// stage's slot), each with its TMA map; outputs are the buffers it writes, each optionally with a contract record.
-#define FE_MAX_SRC 12
+// stage's slot), each with its TMA map in a slab pass; outputs are the buffers it writes, each optionally with a
+// contract record.
+#define FE_MAX_MAP 12   // sources a TMA slab pass stages through shared memory
+#define FE_MAX_SRC 32   // sources a plain pass reads
 #define FE_MAX_OUT 8
 struct FePassArgs {
-    FeTensorMap map[FE_MAX_SRC];
+    FeTensorMap map[FE_MAX_MAP];
     const float* src[FE_MAX_SRC];
     float* out[FE_MAX_OUT];
     FeCheck* rec[FE_MAX_OUT];  // null: this output is not checked in this pass

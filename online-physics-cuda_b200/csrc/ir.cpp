@@ -450,7 +450,7 @@ std::string describe(const Module& m, const law::Law& law)
         else if (in.op == Op::Param) out << ' ' << law.param_names[static_cast<std::size_t>(in.index)];
         for (const int a : in.args) out << " %" << a;
         if (in.op == Op::Shift) out << " (" << in.offset[0] << ',' << in.offset[1] << ',' << in.offset[2] << ')';
-        if (in.op == Op::Tridiag) out << " along " << "xyz"[in.index];
+        if (in.op == Op::Tridiag) out << (in.index >= 3 ? " transposed" : "") << " along " << "xyz"[in.index % 3];
         out << "   [" << (in.shape == Shape::Cell ? "cell" : "scalar");
         if (in.radius > 0) out << ", reads " << in.radius << " away";
         if (m.is_stage(static_cast<int>(i))) out << (in.global ? ", global" : in.net ? ", net" : ", stored");

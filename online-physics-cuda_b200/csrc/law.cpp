@@ -137,6 +137,7 @@ const std::map<std::string, FunctionSpec>& functions()
         {"topple", {Op::Topple, 3, 3}}, {"shift", {Op::Shift, 4, 4}}, {"shift_t", {Op::ShiftT, 4, 4}},
         {"gx_t", {Op::GxT, 1, 1}}, {"gy_t", {Op::GyT, 1, 1}}, {"gz_t", {Op::GzT, 1, 1}},
         {"tridiag_x", {Op::Tridiag, 4, 4}}, {"tridiag_y", {Op::Tridiag, 4, 4}}, {"tridiag_z", {Op::Tridiag, 4, 4}},
+        {"tridiag_x_t", {Op::Tridiag, 4, 4}}, {"tridiag_y_t", {Op::Tridiag, 4, 4}}, {"tridiag_z_t", {Op::Tridiag, 4, 4}},
         {"mlp", {Op::Mlp, 2, 33}}, {"flux", {Op::Flux, 2, 9}}, {"ldiffuse", {Op::LDiffuse, 3, 3}},
     };
     return table;
@@ -295,7 +296,9 @@ private:
         const int id = make(spec.op);
         Node& node = law_.nodes[static_cast<std::size_t>(id)];
         if (spec.op == Op::Tridiag) {
-            node.index = function.back() - 'x';
+            // tridiag_x/_y/_z: axis 0/1/2; the transposed solves tridiag_x_t/_y_t/_z_t (adjoints; not in the
+            // reference's language): 3 + axis.
+            node.index = function[8] - 'x' + (function.size() > 9 ? 3 : 0);
         }
         if (net >= 0) {
             node.index = net;

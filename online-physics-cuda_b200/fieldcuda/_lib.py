@@ -110,6 +110,7 @@ SIGNATURES = {
     "fe_law_destroy": (None, [_p]),
     "fe_law_ir_json": (_i, [_cs, _p, _s, _c.POINTER(_s)]),
     "fe_law_ir_listing": (_i, [_cs, _p, _s, _c.POINTER(_s)]),
+    "fe_law_adjoint": (_i, [_cs, _cs, _p, _s, _c.POINTER(_s)]),
     "fe_law_source": (_i, [_cs, _i, _i, _i, _d, _p, _s, _c.POINTER(_s)]),
     "fe_law_compile_check": (_i, [_cs, _i, _i, _i, _d]),
     "fe_law_field_count": (_i, [_p]),

@@ -153,3 +153,87 @@ def price_at(grid, option):
     ty = min(max(fy - j0, 0.0), 1.0)
     g = grid.astype(np.float64)
     return float((1 - ty) * ((1 - tx) * g[j0, i0] + tx * g[j0, i0 + 1]) + ty * ((1 - tx) * g[j0 + 1, i0] + tx * g[j0 + 1, i0 + 1]))
+
+
+class Calibration:
+    """The Heston calibration's loss and its gradient by reverse mode through the ADI law (the reference's adjoint
+    calibration, bench/calibrate.py, there through the explicit law): the options of one maturity as the z-planes of
+    one (nx, ny) lattice, stepped by tests/laws/heston_douglas.law's scheme (`law_text`), the price read off each plane
+    by the batch's bilinear interpolation, loss = sum (price - target)^2, gradient with respect to (kappa, theta,
+    sigma, rho, v0) through LawSteps (the IR-generated adjoint law, sqrt(N) checkpoints) and torch autograd for the
+    rest (the variance rows sigma (j + 1/2) h and the read-out at v0)."""
+
+    NAMES = ("kappa", "theta", "sigma", "rho", "v0")
+
+    def __init__(self, law_text, strikes, maturity, spot, r, targets, nx, ny, steps):
+        import torch
+        from .adjoint import LawVJP
+        self.n = len(strikes)
+        self.nx, self.ny, self.steps = nx, ny, steps
+        self.h = 6.0 / nx
+        self.dt = maturity / steps
+        self.spot = spot
+        self.r = r
+        self.strikes = np.asarray(strikes, np.float64)
+        self.targets = torch.tensor(np.asarray(targets, np.float64), device="cuda")
+        self.vjp = LawVJP(law_text, nx, ny, self.n, self.h, name="heston_calibration")
+        payoff = np.stack([cell_payoff(k, nx) for k in self.strikes])
+        self.V0 = torch.tensor(np.broadcast_to(payoff[:, None, :], (self.n, ny, nx)).copy(), device="cuda")
+        self.rows = torch.tensor(((np.arange(ny) + 0.5) * self.h)[None, :, None], dtype=torch.float32, device="cuda")
+        x0 = np.log(self.strikes) - 3.0 + 0.5 * self.h
+        self.fx = torch.tensor((np.log(spot) - x0) / self.h, dtype=torch.float64, device="cuda")
+
+    def close(self):
+        self.vjp.close()
+
+    def prices(self, params):
+        """Prices (float64 tensor) of every option under params = (kappa, theta, sigma, rho, v0) tensors."""
+        import torch
+        from .adjoint import LawSteps
+        kappa, theta, sigma, rho, v0 = params
+        shape = (self.n, self.ny, self.nx)
+        f32 = torch.float32
+        full = lambda v: v.to(f32).reshape(1, 1, 1).expand(shape).contiguous()
+        var = (sigma.to(f32) * self.rows).expand(shape).contiguous()
+        names = ("V", "var", "kappa", "theta", "sig_v", "rho", "r")
+        r = torch.full(shape, self.r, dtype=f32, device="cuda")
+        (VT,) = LawSteps.apply(self.vjp, self.dt, self.steps, names, self.V0, var, full(kappa), full(theta), full(sigma), full(rho), r)
+        fx = self.fx
+        fy = v0.double() / (sigma.double() * self.h) - 0.5
+        i0 = torch.clamp(torch.floor(fx), 0, self.nx - 2).long()
+        j0 = torch.clamp(torch.floor(fy.detach()), 0, self.ny - 2).long().expand(self.n)
+        tx = torch.clamp(fx - i0, 0.0, 1.0)
+        ty = torch.clamp(fy - j0, 0.0, 1.0)
+        z = torch.arange(self.n, device="cuda")
+        U = VT.double()
+        a, b = U[z, j0, i0], U[z, j0, i0 + 1]
+        c, d = U[z, j0 + 1, i0], U[z, j0 + 1, i0 + 1]
+        return (1 - ty) * ((1 - tx) * a + tx * b) + ty * ((1 - tx) * c + tx * d)
+
+    def loss(self, params):
+        p = self.prices(params)
+        return ((p - self.targets) ** 2).sum()
+
+    def loss_and_grad(self, values):
+        """(loss, gradient) at values = (kappa, theta, sigma, rho, v0) floats."""
+        import torch
+        params = [torch.tensor(float(v), dtype=torch.float64, device="cuda", requires_grad=True) for v in values]
+        L = self.loss(params)
+        L.backward()
+        return float(L.detach()), np.array([float(p.grad) for p in params])
+
+    def loss_only(self, values):
+        import torch
+        with torch.no_grad():
+            params = [torch.tensor(float(v), dtype=torch.float64, device="cuda") for v in values]
+            return float(self.loss(params))
+
+
+def calibration_options(n, seed):
+    """The calibration set: n strikes U[80, 120] at one maturity (T = 1, spot 100, r = 0.02), and a seeded ground-truth
+    parameter set (kappa U[0.5, 5], theta U[0.01, 0.1], sigma U[0.1, 1], rho U[-0.9, -0.1], v0 U[0.01, 0.1])."""
+    rng = np.random.default_rng(seed)
+    strikes = rng.uniform(80, 120, n)
+    truth = dict(kappa=rng.uniform(0.5, 5), theta=rng.uniform(0.01, 0.1), sigma=rng.uniform(0.1, 1.0),
+                 rho=rng.uniform(-0.9, -0.1), v0=rng.uniform(0.01, 0.1))
+    return strikes, dict(maturity=1.0, spot=100.0, r=0.02), truth

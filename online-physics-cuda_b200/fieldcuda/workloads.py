@@ -2,8 +2,9 @@
 
 * :func:`heat_law` — the plain conduction law (one field, `diffuse`, `conserves`, `max_dt = 0.4 h^2 / 6 D`).
 * :func:`multifield_law` — a 43-term law over 6 fields: radius-1 stencils (diffuse, lap, gx/gy/gz, shift) and reaction
-  products, its params drawn U[0, 1] from a seed. Laws of this shape are what the reference's world law is (43 terms,
-  SURVEY: `perf.md:15`); this one is generated so it can be made at any size and seed.
+  products, its params drawn U[0, 1] from a seed. The reference's shipped world law has 43 terms
+  (bench/results/perf.md:15); this one is generated so it can be made at any size and seed
+  (tests/laws/multifield43.law is seed 0).
 * :func:`blobs` — the sum of Gaussian blobs the heat workload starts from.
 
 The algorithmic bytes of a multi-field step (Lie splitting forbids fusing terms): for every term, 4 bytes a cell for

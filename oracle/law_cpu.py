@@ -146,6 +146,8 @@ class Evaluator:
             yi = np.clip(np.arange(ny) + dy, 0, ny - 1)
             xi = np.clip(np.arange(nx) + dx, 0, nx - 1)
             return _settle(v[zi][:, yi][:, :, xi])
+        if op in ("shift_t", "gx_t", "gy_t", "gz_t"):
+            return self._transposed(op, ins, self._arr(self(a[0])))
         if op in ("lap", "gx", "gy", "gz"):
             v = self(a[0])
             if _uniform(v):
@@ -198,6 +200,54 @@ class Evaluator:
             else:
                 out = (vzp - vzm) / (h * (zp - zm).astype(np.float64))[:, None, None] if nz > 1 else np.zeros(self.shape)
         return np.where(np.isfinite(out), out, 0.0).astype(F32)
+
+    @staticmethod
+    def _run(n, d):
+        """For each cell j along an axis of n cells, the cells i with clamp(i + d) = j: one run lo..hi (Law.cpp:876-882)."""
+        j = np.arange(n)
+        lo = np.maximum(np.where(j == 0, 0, j - d), 0)
+        hi = np.minimum(np.where(j == n - 1, n - 1, j - d), n - 1)
+        return lo, hi
+
+    def _transposed(self, op, ins, v):
+        """shift_t and gx_t/gy_t/gz_t, what each cell sent to the cells that read it gathered back, summed in double in
+        the reference's loop order (Law.cpp:870-919)."""
+        nz, ny, nx = self.shape
+        h = self.h
+        out = np.zeros(self.shape)
+        if op == "shift_t":
+            dx, dy, dz = ins["offset"]
+            runs = [self._run(n, d) for n, d in ((nz, dz), (ny, dy), (nx, dx))]
+            width = [int(np.max(hi - lo + 1)) if len(lo) else 0 for lo, hi in runs]
+            for kz in range(max(width[0], 0)):
+                zz = runs[0][0] + kz
+                okz = zz <= runs[0][1]
+                for ky in range(max(width[1], 0)):
+                    yy = runs[1][0] + ky
+                    oky = yy <= runs[1][1]
+                    for kx in range(max(width[2], 0)):
+                        xx = runs[2][0] + kx
+                        okx = xx <= runs[2][1]
+                        ok = okz[:, None, None] & oky[None, :, None] & okx[None, None, :]
+                        vals = v[np.clip(zz, 0, nz - 1)][:, np.clip(yy, 0, ny - 1)][:, :, np.clip(xx, 0, nx - 1)]
+                        out = out + np.where(ok, vals, 0.0)
+            return _settle(out.astype(F32))
+        axis = {"gx_t": 2, "gy_t": 1, "gz_t": 0}[op]
+        n = self.shape[axis]
+        q = np.arange(n)
+        span = (np.minimum(q + 1, n - 1) - np.maximum(q - 1, 0)).astype(np.float64)
+        shape = [1, 1, 1]
+        shape[axis] = n
+        with np.errstate(all="ignore"):
+            w = np.where(span.reshape(shape) > 0, v / (h * span.reshape(shape)), 0.0)
+        for d in (1, -1):
+            lo, hi = self._run(n, d)
+            for k in range(int(np.max(hi - lo + 1)) if n else 0):
+                idx = lo + k
+                ok = (idx <= hi).reshape(shape)
+                vals = np.take(w, np.clip(idx, 0, n - 1), axis=axis)
+                out = out + np.where(ok, vals if d > 0 else -vals, 0.0)
+        return _settle(out.astype(F32))
 
     def _active_planes(self, v):
         nz = self.shape[0]
@@ -255,10 +305,22 @@ class Evaluator:
             out += up
         return _settle((-out).astype(F32))
 
-    def _tridiag(self, axis, lo, di, up, rhs):
-        """Thomas' algorithm in double, a line at a time, the edge cell repeating (Law.cpp:1098-1138)."""
+    def _tridiag(self, index, lo, di, up, rhs):
+        """Thomas' algorithm in double, a line at a time, the edge cell repeating (Law.cpp:1098-1138). index 3 + axis:
+        the transposed system (tridiag_x_t, an adjoint op this build adds): below the diagonal the previous cell's up,
+        above it the next cell's lo, the edge cells' folded terms on the diagonal."""
+        axis = index % 3
         L, D, U, R = (np.moveaxis(self._arr(x), 2 - axis, -1) for x in (lo, di, up, rhs))
         n = L.shape[-1]
+        if index >= 3:
+            Lt = np.zeros(L.shape)
+            Ut = np.zeros(L.shape)
+            Dt = D.copy()
+            Lt[..., 1:] = U[..., :-1]
+            Ut[..., :-1] = L[..., 1:]
+            Dt[..., 0] = Dt[..., 0] + L[..., 0]
+            Dt[..., n - 1] = Dt[..., n - 1] + U[..., n - 1]
+            L, D, U = Lt, Dt, Ut
         c = np.zeros(L.shape)
         d = np.zeros(L.shape)
         for i in range(n):

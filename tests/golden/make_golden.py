@@ -86,6 +86,14 @@ def cases():
     f, h = heston_fields(32, 16, 3, 7)
     out.append(dict(name="heston_douglas", law="heston_douglas.law", shape=(3, 16, 32), h=h, dt=0.01, steps=4, fields=f))
     out.append(dict(name="heston_hv", law="heston_hv.law", shape=(3, 16, 32), h=h, dt=0.01, steps=4, fields=f))
+    n = (6, 9, 11)
+    rngt = np.random.default_rng(7)
+    out.append(dict(name="ops_transposed", law="ops_transposed.law", shape=n, h=0.5, dt=0.01, steps=3,
+                    fields={"a": rngt.uniform(-1, 1, n).astype(np.float32), "b": rngt.uniform(-1, 1, n).astype(np.float32)}))
+    n = (12, 16, 20)
+    rngm = np.random.default_rng(43)
+    out.append(dict(name="multifield43", law="multifield43.law", shape=n, h=1.0 / 20, dt=0.1 * (1.0 / 20) ** 2, steps=3,
+                    fields={f"f{i}": rngm.uniform(-1, 1, n).astype(np.float32) for i in range(6)}))
     out.append(dict(name="heston_explicit", law="heston_explicit.law", shape=(3, 16, 32), h=h, dt=0.01, steps=3, fields=f))
     return out
 
