@@ -230,6 +230,33 @@ int fe_heston_batch_time(fe_heston_batch* batch, int use_graph, float* ms);
 int fe_heston_batch_prices(fe_heston_batch* batch, float* host_prices);
 int fe_heston_batch_grid(fe_heston_batch* batch, int option, float* host_grid);
 
+/* ---- learned coarse-lattice correction on the tensor cores ----------------------------------------------------------------
+ * A small network applied per cell of a coarse 2-D lattice (each z-plane a sample) after the plain law's step: the 3 x 3
+ * neighbourhood of (u, v), edge repeating, -> 64 (ReLU) -> 64 (ReLU) -> 2, added to (u, v): a 3x3 convolution, then two
+ * pointwise layers, BF16 on the tensor cores (tcgen05) with FP32 accumulation, trained by the library's own forward and
+ * backward kernels (loss 1/2 mean over cells of the squared error against a target state; Adam on FP32 masters). It
+ * replaces the reference's fp16 mma.sync net stages (src/field/cuda/CudaNet.cpp:175-369) for this form; the plain fine
+ * law stays the judge, and fe_corr_apply is guarded: the corrected state replaces the plain step's only if every cell is
+ * finite and within [lo, hi] (decided on the card). Weights are fe_corr_weight_count() floats: W1 (32 x 64) | W2 (80 x 64)
+ * | W3 (80 x 16), row-major, rows = inputs (W1 rows 0..17 the neighbourhood as (u, v) pairs row by row, row 18 the bias;
+ * W2, W3 row 64 the bias; other rows, and W3 columns past 1, zero). Device pointers are float32 nx * ny * nz lattices;
+ * `stream` is a cudaStream_t (NULL: the legacy stream). */
+typedef struct fe_corrector fe_corrector;
+int fe_corr_create(fe_corrector** out);
+void fe_corr_destroy(fe_corrector* corr);
+int fe_corr_weight_count(void);
+int fe_corr_set_weights(fe_corrector* corr, const float* host_weights);
+int fe_corr_get_weights(fe_corrector* corr, float* host_weights);
+/* The loss and its gradient (host_grads may be NULL) of the network on (u, v) against (target_u, target_v). */
+int fe_corr_grads(fe_corrector* corr, const float* u, const float* v, const float* target_u, const float* target_v, int nx, int ny,
+                  int nz, void* stream, double* host_loss, float* host_grads);
+/* One Adam step (learning rate lr) on that gradient; host_loss (may be NULL) is the loss before the step. */
+int fe_corr_train_step(fe_corrector* corr, const float* u, const float* v, const float* target_u, const float* target_v, int nx,
+                       int ny, int nz, void* stream, float lr, double* host_loss);
+/* (u, v) += the network's correction, in place, guarded; *reverted (may be NULL: no wait for the verdict) is 1 when the
+ * plain step's state was kept. */
+int fe_corr_apply(fe_corrector* corr, float* u, float* v, int nx, int ny, int nz, float lo, float hi, void* stream, int* reverted);
+
 #ifdef __cplusplus
 }
 #endif

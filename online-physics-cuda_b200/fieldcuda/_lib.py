@@ -148,6 +148,14 @@ SIGNATURES = {
     "fe_heston_batch_time": (_i, [_p, _i, _c.POINTER(_c.c_float)]),
     "fe_heston_batch_prices": (_i, [_p, _p]),
     "fe_heston_batch_grid": (_i, [_p, _i, _p]),
+    "fe_corr_create": (_i, [_c.POINTER(_p)]),
+    "fe_corr_destroy": (None, [_p]),
+    "fe_corr_weight_count": (_i, []),
+    "fe_corr_set_weights": (_i, [_p, _p]),
+    "fe_corr_get_weights": (_i, [_p, _p]),
+    "fe_corr_grads": (_i, [_p, _p, _p, _p, _p, _i, _i, _i, _p, _c.POINTER(_d), _p]),
+    "fe_corr_train_step": (_i, [_p, _p, _p, _p, _p, _i, _i, _i, _p, _c.c_float, _c.POINTER(_d)]),
+    "fe_corr_apply": (_i, [_p, _p, _p, _i, _i, _i, _c.c_float, _c.c_float, _p, _c.POINTER(_i)]),
 }
 
 
