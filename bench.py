@@ -430,6 +430,99 @@ def calibration_section():
             "what": "wall clock of one loss + gradient (forward, checkpointed recompute, adjoint law backward)"}
 
 
+FHN_LAW = os.path.join(ROOT, "tests", "laws", "fhn_rk4.law")
+FHN_TRUTH = os.path.join(ROOT, "tests", "golden", "fhn", "truth.npz")
+
+
+def fhn_learned_section(samples=1000, frames=100, train_samples=64, iters=3000):
+    """FitzHugh-Nagumo (u, v) on [-1, 1]^2, t in [0, 5] in 100 frames of 0.05, N(0, 1) starts per cell (seeded), as
+    z-planes of one lattice: the learned form (32 x 32 plain law + the tensor-core correction after every frame,
+    trained here on the engine's own 128 x 128 solves of 64 other seeds) against the plain law at 32, 64 and 128.
+    Errors (RMSE of (u, v) averaged onto 32 x 32, every 10th frame) against the plain 128 x 128 solve (the judge) and,
+    for the first 4 seeds, against an FP64 method-of-lines solve (tests/golden/fhn/truth.npz). solves/s = samples over
+    the device time of the 100 frames."""
+    import numpy as np
+    import torch
+    import torch.nn.functional as F
+    from fieldcuda.learned import Corrector, PlainFHN, block_mean, fhn_initial, fine_frames, init_weights, train_correction
+
+    text = open(FHN_LAW).read()
+
+    def pool(x, f):
+        return F.avg_pool2d(x[:, None], f)[:, 0].contiguous() if f > 1 else x
+
+    t0 = time.perf_counter()
+    targets = fine_frames(text, list(range(train_samples)), frames)
+    torch.cuda.synchronize()
+    data_s = time.perf_counter() - t0
+    corr = Corrector(init_weights(7))
+    t0 = time.perf_counter()
+    train_rmse, train_plain_rmse = train_correction(corr, text, targets, iters=iters, rounds=2)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    seeds = list(range(1000, 1000 + samples))
+    su, sv = fhn_initial(seeds, 128)
+    keep = list(range(10, frames + 1, 10))
+
+    def run(n, learned, snapshots):
+        s = PlainFHN(text, n, samples)
+        f = 128 // n
+        s.set(block_mean(su, f) if f > 1 else su, block_mean(sv, f) if f > 1 else sv)
+        st = torch.cuda.ExternalStream(s.solver.stream)
+        snaps = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        for t in range(1, frames + 1):
+            s.step()
+            if learned:
+                corr.apply_solver(s.solver, time=t * s.frame)
+            if snapshots and t in keep:
+                u, v = s.get()
+                snaps.append((pool(u, n // 32), pool(v, n // 32)))
+        e1.record(st)
+        st.synchronize()
+        ms = e0.elapsed_time(e1)
+        subs = s.substeps()
+        s.solver.sync()
+        broken = len(s.solver.violations())
+        s.close()
+        return ms, snaps, subs, broken
+
+    methods = {"plain_32": (32, False), "plain_64": (64, False), "plain_128": (128, False), "learned_32": (32, True)}
+    out = {}
+    snaps = {}
+    for name, (n, learned) in methods.items():
+        run(n, learned, False)
+        ms, _, subs, broken = run(n, learned, False)
+        _, snaps[name], _, _ = run(n, learned, True)
+        out[name] = {"lattice": f"{n} x {n} x {samples}", "substeps_per_frame": subs, "ms": ms,
+                     "solves_per_s": samples / (ms * 1e-3), "violations": broken}
+    judge = snaps["plain_128"]
+    truth = np.load(FHN_TRUTH)["states"] if os.path.exists(FHN_TRUTH) else None
+    for name in methods:
+        err = [float(((a - ja) ** 2 + (b - jb) ** 2).mean() / 2) for (a, b), (ja, jb) in zip(snaps[name], judge)]
+        out[name]["rmse_vs_plain_128"] = float(np.sqrt(np.mean(err)))
+        if truth is not None:
+            e64 = []
+            for k, (a, b) in enumerate(snaps[name]):
+                ref = truth[k + 1]
+                e64.append(float((((a[:4].cpu().numpy() - ref[0]) ** 2 + (b[:4].cpu().numpy() - ref[1]) ** 2) / 2).mean()))
+            out[name]["rmse_vs_fp64_4_seeds"] = float(np.sqrt(np.mean(e64)))
+    corr.close()
+    learned_err = out["learned_32"]["rmse_vs_plain_128"]
+    matches = [m for m in ("plain_32", "plain_64", "plain_128") if out[m]["rmse_vs_plain_128"] <= learned_err]
+    equal = matches[0] if matches else None
+    return {"samples": samples, "frames": frames, "methods": out,
+            "training": {"seeds": train_samples, "pairs": frames, "adam_steps": iters * 3, "rounds": "teacher forcing, then 2 rounds on "
+                         "the learned solver's own rollouts", "seconds": train_s, "data_seconds": data_s,
+                         "rollout_rmse_train": train_rmse, "plain_rollout_rmse_train": train_plain_rmse},
+            "equal_error_plain": equal,
+            "speedup_at_equal_error": (out["learned_32"]["solves_per_s"] / out[equal]["solves_per_s"]) if equal else None,
+            "network": "3x3 conv of (u, v) and the time 2->64, ReLU, 64->64, ReLU, 64->2, BF16 tcgen05, FP32 accumulators "
+                       "(10,752 FLOP a cell)"}
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -530,6 +623,9 @@ def run_ours(args, world, rank, local):
     calibration = None
     if not args.no_calibration:
         calibration = calibration_section()
+    learned = None
+    if not args.no_learned:
+        learned = fhn_learned_section()
 
     if rank != 0:
         return
@@ -557,6 +653,7 @@ def run_ours(args, world, rank, local):
         "heston_batch": heston,
         "multifield_256": multifield,
         "adjoint_calibration": calibration,
+        "fhn_learned": learned,
     }))
 
 
@@ -571,6 +668,7 @@ def main():
     ap.add_argument("--no-heston", action="store_true", help="skip the batched Heston ADI section")
     ap.add_argument("--no-multifield", action="store_true", help="skip the 43-term multi-field law section")
     ap.add_argument("--no-calibration", action="store_true", help="skip the adjoint calibration section")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-correction section")
     args = ap.parse_args()
     world, rank, local = init_dist()
     try:

@@ -167,6 +167,10 @@ int fe_law_upload_device(fe_law* law, int field, const float* dev);
 int fe_law_fetch(fe_law* law, int field, float* host);
 int fe_law_fetch_device(fe_law* law, int field, float* dev);
 /* The card's current buffer of a field (valid until the next step). */
+/* The field's current device buffer was changed in place by the caller, on the handle's stream (fe_law_stream) after
+ * its last step: the backend forgets what it knew of the field's bounds (no counterpart in the reference, whose host
+ * FieldSet is written through FieldEdits instead). */
+int fe_law_mark_edited(fe_law* law, int field);
 int fe_law_field_device_ptr(const fe_law* law, int field, const float** dev);
 
 /* One step of dt: every term in declaration order with its substeps, then the derives (Solver::step,
@@ -238,9 +242,10 @@ int fe_heston_batch_grid(fe_heston_batch* batch, int option, float* host_grid);
  * replaces the reference's fp16 mma.sync net stages (src/field/cuda/CudaNet.cpp:175-369) for this form; the plain fine
  * law stays the judge, and fe_corr_apply is guarded: the corrected state replaces the plain step's only if every cell is
  * finite and within [lo, hi] (decided on the card). Weights are fe_corr_weight_count() floats: W1 (32 x 64) | W2 (80 x 64)
- * | W3 (80 x 16), row-major, rows = inputs (W1 rows 0..17 the neighbourhood as (u, v) pairs row by row, row 18 the bias;
- * W2, W3 row 64 the bias; other rows, and W3 columns past 1, zero). Device pointers are float32 nx * ny * nz lattices;
- * `stream` is a cudaStream_t (NULL: the legacy stream). */
+ * | W3 (80 x 16), row-major, rows = inputs (W1 rows 0..17 the neighbourhood as (u, v) pairs row by row, row 18 the bias,
+ * row 19 the `time` input; W2, W3 row 64 the bias; other rows, and W3 columns past 1, zero). `time` is the time since the
+ * start of the solve of the state being corrected. Device pointers are float32 nx * ny * nz lattices; `stream` is a
+ * cudaStream_t (NULL: the legacy stream). */
 typedef struct fe_corrector fe_corrector;
 int fe_corr_create(fe_corrector** out);
 void fe_corr_destroy(fe_corrector* corr);
@@ -249,13 +254,14 @@ int fe_corr_set_weights(fe_corrector* corr, const float* host_weights);
 int fe_corr_get_weights(fe_corrector* corr, float* host_weights);
 /* The loss and its gradient (host_grads may be NULL) of the network on (u, v) against (target_u, target_v). */
 int fe_corr_grads(fe_corrector* corr, const float* u, const float* v, const float* target_u, const float* target_v, int nx, int ny,
-                  int nz, void* stream, double* host_loss, float* host_grads);
+                  int nz, float time, void* stream, double* host_loss, float* host_grads);
 /* One Adam step (learning rate lr) on that gradient; host_loss (may be NULL) is the loss before the step. */
 int fe_corr_train_step(fe_corrector* corr, const float* u, const float* v, const float* target_u, const float* target_v, int nx,
-                       int ny, int nz, void* stream, float lr, double* host_loss);
+                       int ny, int nz, float time, void* stream, float lr, double* host_loss);
 /* (u, v) += the network's correction, in place, guarded; *reverted (may be NULL: no wait for the verdict) is 1 when the
  * plain step's state was kept. */
-int fe_corr_apply(fe_corrector* corr, float* u, float* v, int nx, int ny, int nz, float lo, float hi, void* stream, int* reverted);
+int fe_corr_apply(fe_corrector* corr, float* u, float* v, int nx, int ny, int nz, float time, float lo, float hi, void* stream,
+                  int* reverted);
 
 #ifdef __cplusplus
 }

@@ -234,6 +234,13 @@ int fe_law_fetch_device(fe_law* law, int field, float* dev)
     return fe::ok();
 }
 
+int fe_law_mark_edited(fe_law* law, int field)
+{
+    if (!field_ok(law, field)) return fe::fail(FE_EINVAL, "bad field");
+    law->engine.mark_edited(field);
+    return fe::ok();
+}
+
 int fe_law_field_device_ptr(const fe_law* law, int field, const float** dev)
 {
     if (!field_ok(law, field) || dev == nullptr) return fe::fail(FE_EINVAL, "bad field");

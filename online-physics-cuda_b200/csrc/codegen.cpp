@@ -467,7 +467,9 @@ private:
             rz = std::max(rz, pb.reach[k].z);
         }
         L.rz = rz;
-        if ((nx_ % 4) != 0 || pb.sources.empty() || pb.sources.size() > FE_MAX_MAP_HOST) return false;
+        // A slab tile is 128 cells wide: a lattice narrower than that would leave most of each tile's lanes idle and
+        // stage a plane a CTA, so it takes the plain pass (a thread a cell, as many CTAs as the planes allow).
+        if ((nx_ % 4) != 0 || nx_ < 128 || pb.sources.empty() || pb.sources.size() > FE_MAX_MAP_HOST) return false;
         for (const Source& s : pb.sources) {
             if (128 + 2 * s.ax > 256 || s.ry > 64) return false;
         }

@@ -2,10 +2,11 @@
 // accumulators in tensor memory, inference and training (forward and backward) in one hand-written kernel.
 //
 // The network, per cell of a coarse 2-D lattice (every z-plane a sample): the 3 x 3 neighbourhood of (u, v) with the
-// edge cell repeating (18 numbers) -> 64 (ReLU) -> 64 (ReLU) -> 2, the correction added to the state the plain coarse
-// step left: a 3x3 convolution with 2 input and 64 output channels, then two pointwise (1x1) layers. Biases are rows of
-// the weight matrices fed by a constant-1 input feature (input 18 of layer 1, feature 64 of the hidden layers), so each
-// layer is one GEMM over 128-cell tiles: Z1 = X0 W1 (K 32), Z2 = H1 W2 (K 80), Y = H2 W3 (K 80, N 16 of which 2 used).
+// edge cell repeating (18 numbers) and the time since the start of the solve -> 64 (ReLU) -> 64 (ReLU) -> 2, the
+// correction added to the state the plain coarse step left: a 3x3 convolution with 2 input and 64 output channels (and
+// the time), then two pointwise (1x1) layers. Biases are rows of the weight matrices fed by a constant-1 input feature
+// (input 18 of layer 1, feature 64 of the hidden layers), so each layer is one GEMM over 128-cell tiles: Z1 = X0 W1
+// (K 32), Z2 = H1 W2 (K 80), Y = H2 W3 (K 80, N 16 of which 2 used).
 //
 // Layout: every operand is a 128-row (cells) or in-feature-row matrix of BF16 in the canonical no-swizzle core-matrix
 // layout (8 rows x 16 bytes a core matrix, element (r, c) at ((c/8) (R/8) + r/8) 128 + (r%8) 16 + (c%8) 2 bytes). The
@@ -68,6 +69,7 @@ struct CorrArgs {
     int nx, ny, nz;
     long long cells;
     float lo, hi;
+    float time;          // the time since the start of the solve: input 19 of every cell
 };
 
 __host__ __device__ constexpr unsigned core_off(int r, int c, int R)
@@ -248,6 +250,7 @@ __global__ void __launch_bounds__(kThreadsC, 1) corr_kernel(const CorrArgs a)
                 }
             }
             x0[18] = 1.f;
+            x0[19] = a.time;
             uc = x0[8];
             vc = x0[9];
         }
@@ -290,7 +293,7 @@ __global__ void __launch_bounds__(kThreadsC, 1) corr_kernel(const CorrArgs a)
         float y[16];
         tld16(lane_base + kTY, y);
         tld_wait();
-        if (!TRAIN) {
+        if constexpr (!TRAIN) {
             if (valid) {
                 const float nu = uc + y[0], nv = vc + y[1];
                 const bool in = nu == nu && nv == nv && nu >= a.lo && nu <= a.hi && nv >= a.lo && nv <= a.hi;
@@ -301,7 +304,7 @@ __global__ void __launch_bounds__(kThreadsC, 1) corr_kernel(const CorrArgs a)
             tc_before();
             __syncthreads();
             continue;
-        }
+        } else {
         // 4. Backward: dY, then dH2 = dY W3^T and dW3 += H2^T dY.
         float dy[16];
 #pragma unroll
@@ -354,9 +357,10 @@ __global__ void __launch_bounds__(kThreadsC, 1) corr_kernel(const CorrArgs a)
         if (!(ok = mma_wait(bar, phase, a.err))) break;
         tc_before();
         __syncthreads();
+        }
     }
 
-    if (TRAIN) {
+    if constexpr (TRAIN) {
         // This CTA's weight gradients out of tensor memory (rows = TMEM lanes), and its share of the loss.
         float* g = a.gpart + static_cast<long long>(blockIdx.x) * kWeights;
         const int row = t;
@@ -411,7 +415,7 @@ __global__ void corr_commit(const float* ou, const float* ov, float* u, float* v
 }
 
 // Fixed-order sum of the CTAs' gradients, then Adam on the FP32 masters; the BF16 copy is rewritten in its core layout.
-// Padding rows and columns (inputs 19..31 of W1, 65..79 of W2 and W3, outputs 2..15 of W3) stay zero.
+// Padding rows and columns (inputs 20..31 of W1, 65..79 of W2 and W3, outputs 2..15 of W3) stay zero.
 __global__ void corr_adam(float* w, float* m, float* v2, unsigned short* wb, const float* gpart, int parts, float scale, float lr,
     float b1t, float b2t, float* grad_out)
 {
@@ -423,7 +427,7 @@ __global__ void corr_adam(float* w, float* m, float* v2, unsigned short* wb, con
     else { rows = 80; cols = 16; off = kW1 + kW2; }
     r = (i - off) / cols;
     c = (i - off) - r * cols;
-    const bool pad = (off == 0 && r > 18) || (off != 0 && r > 64) || (off == kW1 + kW2 && c > 1);
+    const bool pad = (off == 0 && r > 19) || (off != 0 && r > 64) || (off == kW1 + kW2 && c > 1);
     double g = 0.0;
     for (int p = 0; p < parts; ++p) g += gpart[static_cast<long long>(p) * kWeights + i];
     const float gs = pad ? 0.f : static_cast<float>(g) * scale;
@@ -491,8 +495,8 @@ fe::CorrArgs base_args(fe_corrector* c, int nx, int ny, int nz)
     return a;
 }
 
-int run_grads(fe_corrector* c, const float* u, const float* v, const float* tu, const float* tv, int nx, int ny, int nz, cudaStream_t s,
-    float lr, double* host_loss, float* host_grads)
+int run_grads(fe_corrector* c, const float* u, const float* v, const float* tu, const float* tv, int nx, int ny, int nz, float time,
+    cudaStream_t s, float lr, double* host_loss, float* host_grads)
 {
     std::string why;
     if (!c || !u || !v || !tu || !tv || nx < 1 || ny < 1 || nz < 1) return fe::fail(FE_EINVAL, "corrector: bad arguments");
@@ -501,6 +505,7 @@ int run_grads(fe_corrector* c, const float* u, const float* v, const float* tu, 
     a.v = v;
     a.tu = tu;
     a.tv = tv;
+    a.time = time;
     const long long tiles = (a.cells + fe::kTile - 1) / fe::kTile;
     const int grid = static_cast<int>(std::min<long long>(tiles, c->ctas));
     if (!fe::cuda_ok(cudaMemsetAsync(c->err, 0, 4 * sizeof(unsigned), s), "reset", why)) return fe::fail(FE_ECUDA, why);
@@ -602,20 +607,20 @@ int fe_corr_get_weights(fe_corrector* c, float* host_w)
     return fe::ok();
 }
 
-int fe_corr_grads(fe_corrector* c, const float* u, const float* v, const float* tu, const float* tv, int nx, int ny, int nz, void* stream,
-    double* host_loss, float* host_grads)
+int fe_corr_grads(fe_corrector* c, const float* u, const float* v, const float* tu, const float* tv, int nx, int ny, int nz, float time,
+    void* stream, double* host_loss, float* host_grads)
 {
-    return run_grads(c, u, v, tu, tv, nx, ny, nz, static_cast<cudaStream_t>(stream), 0.f, host_loss, host_grads);
+    return run_grads(c, u, v, tu, tv, nx, ny, nz, time, static_cast<cudaStream_t>(stream), 0.f, host_loss, host_grads);
 }
 
-int fe_corr_train_step(fe_corrector* c, const float* u, const float* v, const float* tu, const float* tv, int nx, int ny, int nz, void* stream,
-    float lr, double* host_loss)
+int fe_corr_train_step(fe_corrector* c, const float* u, const float* v, const float* tu, const float* tv, int nx, int ny, int nz, float time,
+    void* stream, float lr, double* host_loss)
 {
     if (!(lr > 0.f)) return fe::fail(FE_EINVAL, "learning rate must be positive");
-    return run_grads(c, u, v, tu, tv, nx, ny, nz, static_cast<cudaStream_t>(stream), lr, host_loss, nullptr);
+    return run_grads(c, u, v, tu, tv, nx, ny, nz, time, static_cast<cudaStream_t>(stream), lr, host_loss, nullptr);
 }
 
-int fe_corr_apply(fe_corrector* c, float* u, float* v, int nx, int ny, int nz, float lo, float hi, void* stream, int* reverted)
+int fe_corr_apply(fe_corrector* c, float* u, float* v, int nx, int ny, int nz, float time, float lo, float hi, void* stream, int* reverted)
 {
     std::string why;
     if (!c || !u || !v || nx < 1 || ny < 1 || nz < 1) return fe::fail(FE_EINVAL, "corrector: bad arguments");
@@ -628,6 +633,7 @@ int fe_corr_apply(fe_corrector* c, float* u, float* v, int nx, int ny, int nz, f
     a.ov = c->ov;
     a.lo = lo;
     a.hi = hi;
+    a.time = time;
     const long long tiles = (a.cells + fe::kTile - 1) / fe::kTile;
     const int grid = static_cast<int>(std::min<long long>(tiles, c->ctas));
     if (!fe::cuda_ok(cudaMemsetAsync(c->err, 0, 4 * sizeof(unsigned), s), "reset", why)) return fe::fail(FE_ECUDA, why);

@@ -328,6 +328,13 @@ bool Engine::upload(int field, const void* src, bool device, std::string& why)
     return true;
 }
 
+void Engine::mark_edited(int field)
+{
+    if (field < 0 || static_cast<std::size_t>(field) >= now_.size()) return;
+    bounds_[static_cast<std::size_t>(field)] = Bounds{};
+    zero_[static_cast<std::size_t>(field)] = 0;
+}
+
 bool Engine::fetch(int field, void* dst, bool device, std::string& why)
 {
     if (field < 0 || static_cast<std::size_t>(field) >= now_.size()) {
@@ -341,10 +348,19 @@ bool Engine::fetch(int field, void* dst, bool device, std::string& why)
 
 // ---- the idle-term test (LawBounds.cpp:13-213 over the IR) ---------------------------------------------------------------
 
+// One forward pass over the instructions up to `id` (every argument has a lower id than its user), so a value the
+// law reuses through lets is bounded once, not once per path to it.
 Bounds Engine::bounds_of(int id, const std::vector<Bounds>& fields) const
 {
+    std::vector<Bounds> memo(static_cast<std::size_t>(id) + 1);
+    for (int i = 0; i <= id; ++i) memo[static_cast<std::size_t>(i)] = bounds_one(i, fields, memo);
+    return memo[static_cast<std::size_t>(id)];
+}
+
+Bounds Engine::bounds_one(int id, const std::vector<Bounds>& fields, const std::vector<Bounds>& memo) const
+{
     const ir::Inst& in = mod_.insts[static_cast<std::size_t>(id)];
-    auto arg = [&](std::size_t i) { return bounds_of(in.args[i], fields); };
+    auto arg = [&](std::size_t i) { return memo[static_cast<std::size_t>(in.args[i])]; };
     auto clean = [](double lo, double hi) {
         return Bounds{std::isnan(lo) ? -std::numeric_limits<double>::infinity() : lo, std::isnan(hi) ? std::numeric_limits<double>::infinity() : hi};
     };
@@ -414,8 +430,15 @@ Bounds Engine::bounds_of(int id, const std::vector<Bounds>& fields) const
 
 bool Engine::always_zero(int id) const
 {
+    std::vector<char> memo(static_cast<std::size_t>(id) + 1, 0);
+    for (int i = 0; i <= id; ++i) memo[static_cast<std::size_t>(i)] = zero_one(i, memo) ? 1 : 0;
+    return memo[static_cast<std::size_t>(id)] != 0;
+}
+
+bool Engine::zero_one(int id, const std::vector<char>& memo) const
+{
     const ir::Inst& in = mod_.insts[static_cast<std::size_t>(id)];
-    auto arg = [&](std::size_t i) { return always_zero(in.args[i]); };
+    auto arg = [&](std::size_t i) { return memo[static_cast<std::size_t>(in.args[i])] != 0; };
     switch (in.op) {
     case Op::Const: return in.number == 0.0;
     case Op::Param: return law_.param_values[static_cast<std::size_t>(in.index)] == 0.0;

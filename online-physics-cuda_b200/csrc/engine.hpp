@@ -50,6 +50,9 @@ public:
 
     // Host <-> card.
     bool upload(int field, const void* src, bool device, std::string& why);
+    // A field's cells were changed in place on the device by someone else (ordered on the engine's stream): what the
+    // engine knew of its bounds no longer holds.
+    void mark_edited(int field);
     bool fetch(int field, void* dst, bool device, std::string& why);
     const float* device_field(int field) const { return now_[static_cast<std::size_t>(field)]; }
 
@@ -108,7 +111,9 @@ private:
     double scalar_value(int id, bool& ok, std::string& why);
     bool idle(const ir::Program& p) const;
     Bounds bounds_of(int id, const std::vector<Bounds>& fields) const;
+    Bounds bounds_one(int id, const std::vector<Bounds>& fields, const std::vector<Bounds>& memo) const;
     bool always_zero(int id) const;
+    bool zero_one(int id, const std::vector<char>& memo) const;
     void flow_bounds(const ir::Program& p, double dt, int substeps);
 
     law::Law law_;

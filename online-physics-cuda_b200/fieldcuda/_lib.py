@@ -128,6 +128,7 @@ SIGNATURES = {
     "fe_law_fetch": (_i, [_p, _i, _p]),
     "fe_law_fetch_device": (_i, [_p, _i, _p]),
     "fe_law_field_device_ptr": (_i, [_p, _i, _c.POINTER(_p)]),
+    "fe_law_mark_edited": (_i, [_p, _i]),
     "fe_law_step": (_i, [_p, _d, _i, _c.POINTER(fe_step_info)]),
     "fe_law_derive": (_i, [_p]),
     "fe_law_check_every": (_i, [_p, _i]),
@@ -153,9 +154,9 @@ SIGNATURES = {
     "fe_corr_weight_count": (_i, []),
     "fe_corr_set_weights": (_i, [_p, _p]),
     "fe_corr_get_weights": (_i, [_p, _p]),
-    "fe_corr_grads": (_i, [_p, _p, _p, _p, _p, _i, _i, _i, _p, _c.POINTER(_d), _p]),
-    "fe_corr_train_step": (_i, [_p, _p, _p, _p, _p, _i, _i, _i, _p, _c.c_float, _c.POINTER(_d)]),
-    "fe_corr_apply": (_i, [_p, _p, _p, _i, _i, _i, _c.c_float, _c.c_float, _p, _c.POINTER(_i)]),
+    "fe_corr_grads": (_i, [_p, _p, _p, _p, _p, _i, _i, _i, _c.c_float, _p, _c.POINTER(_d), _p]),
+    "fe_corr_train_step": (_i, [_p, _p, _p, _p, _p, _i, _i, _i, _c.c_float, _p, _c.c_float, _c.POINTER(_d)]),
+    "fe_corr_apply": (_i, [_p, _p, _p, _i, _i, _i, _c.c_float, _c.c_float, _c.c_float, _p, _c.POINTER(_i)]),
 }
 
 

@@ -122,6 +122,10 @@ class Solver:
         _lib.check(self._lib.fe_law_fetch(self._h, self._id(field), out.ctypes.data_as(ctypes.c_void_p)))
         return out
 
+    def mark_edited(self, field):
+        """The field's device buffer (device_ptr) was changed in place on this solver's stream."""
+        _lib.check(self._lib.fe_law_mark_edited(self._h, self._id(field)))
+
     def fetch_device(self, field, tensor):
         _lib.check(self._lib.fe_law_fetch_device(self._h, self._id(field), ctypes.c_void_p(tensor.data_ptr())))
 

@@ -2,7 +2,7 @@
 online-physics-cuda_b200/csrc/corrector.cu, never on a product path).
 
 The network and its operands follow the kernel's definition: per cell the 3 x 3 neighbourhood of (u, v), edge
-repeating, as 18 inputs plus a constant 1 (bias), -> 64 ReLU (+ constant 1) -> 64 ReLU (+ constant 1) -> 2, the output
+repeating, as 18 inputs plus a constant 1 (bias) and the time, -> 64 ReLU (+ constant 1) -> 64 ReLU (+ constant 1) -> 2, the output
 added to (u, v) at the cell. Every matrix operand is rounded to bfloat16 (round to nearest even) where the kernel stores
 it in shared memory — the inputs, the weights, the hidden activations, dY and the dZs — and every product is
 accumulated in float64 here (the tensor cores accumulate in FP32, so the two agree to FP32 rounding of the sums).
@@ -37,8 +37,9 @@ def unpack(w):
     return w[:o1].reshape(W1_SHAPE), w[o1:o2].reshape(W2_SHAPE), w[o2:].reshape(W3_SHAPE)
 
 
-def features(u, v):
-    """(cells, 32): the 3 x 3 neighbourhood of (u, v) per cell, (dy, dx) row by row as (u, v) pairs, the constant 1 at 18."""
+def features(u, v, time=0.0):
+    """(cells, 32): the 3 x 3 neighbourhood of (u, v) per cell, (dy, dx) row by row as (u, v) pairs, the constant 1 at 18,
+    the time at 19."""
     nz, ny, nx = u.shape
     feats = np.zeros((nz, ny, nx, 32), np.float32 if ROUND else np.float64)
     ys, xs = np.arange(ny), np.arange(nx)
@@ -50,13 +51,14 @@ def features(u, v):
             feats[..., k] = u[:, yy][:, :, xx]
             feats[..., k + 1] = v[:, yy][:, :, xx]
     feats[..., 18] = 1.0
+    feats[..., 19] = time
     return feats.reshape(-1, 32)
 
 
-def forward(w, u, v):
+def forward(w, u, v, time=0.0):
     """The corrections (cells, 2) and the intermediates the backward needs."""
     W1, W2, W3 = (np.asarray(bf16(m), np.float64) for m in unpack(w))
-    X0 = np.asarray(bf16(features(u, v)), np.float64)
+    X0 = np.asarray(bf16(features(u, v, time)), np.float64)
     f = np.float32 if ROUND else np.float64
     Z1 = (X0 @ W1).astype(f)
     H1 = np.zeros((X0.shape[0], 80), np.float64)
@@ -70,15 +72,15 @@ def forward(w, u, v):
     return Y[:, :2], dict(X0=X0, Z1=Z1, H1=H1, Z2=Z2, H2=H2, W1=W1, W2=W2, W3=W3)
 
 
-def apply(w, u, v):
-    y, _ = forward(w, u, v)
+def apply(w, u, v, time=0.0):
+    y, _ = forward(w, u, v, time)
     shape = u.shape
     return (u.reshape(-1) + y[:, 0]).reshape(shape), (v.reshape(-1) + y[:, 1]).reshape(shape)
 
 
-def loss_and_grads(w, u, v, tu, tv):
+def loss_and_grads(w, u, v, tu, tv, time=0.0):
     """(loss, flat gradient of 8448 floats) of 1/2 mean squared error of (u, v) + correction against (tu, tv)."""
-    y, c = forward(w, u, v)
+    y, c = forward(w, u, v, time)
     n = y.shape[0]
     f = np.float32 if ROUND else np.float64
     pu = u.reshape(-1).astype(f) + y[:, 0]
@@ -102,9 +104,9 @@ def loss_and_grads(w, u, v, tu, tv):
 
 
 def pad_mask():
-    """True where a weight is padding that stays zero (W1 inputs past 18; W2, W3 inputs past 64; W3 outputs past 1)."""
+    """True where a weight is padding that stays zero (W1 inputs past 19; W2, W3 inputs past 64; W3 outputs past 1)."""
     m1 = np.zeros(W1_SHAPE, bool)
-    m1[19:] = True
+    m1[20:] = True
     m2 = np.zeros(W2_SHAPE, bool)
     m2[65:] = True
     m3 = np.zeros(W3_SHAPE, bool)

@@ -39,8 +39,8 @@ def test_forward_matches_the_oracle(cuda, shape):
     u, v, w = random_case(shape, 1)
     c = Corrector(w)
     U, V = tensors(u, v)
-    assert c.apply(U, V, -1e30, 1e30) is False
-    want_u, want_v = net_cpu.apply(w, u, v)
+    assert c.apply(U, V, -1e30, 1e30, time=0.75) is False
+    want_u, want_v = net_cpu.apply(w, u, v, time=0.75)
     du_g, du_w = U.cpu().numpy() - u, want_u - u
     dv_g, dv_w = V.cpu().numpy() - v, want_v - v
     scale = max(np.abs(du_w).max(), np.abs(dv_w).max())
@@ -59,8 +59,8 @@ def test_loss_and_gradients_match_the_oracle(cuda):
     tu = (u + 0.3 * rng.normal(size=shape)).astype(np.float32)
     tv = (v + 0.3 * rng.normal(size=shape)).astype(np.float32)
     c = Corrector(w)
-    loss, g = c.grads(*tensors(u, v, tu, tv))
-    want_loss, want_g = net_cpu.loss_and_grads(w, u, v, tu, tv)
+    loss, g = c.grads(*tensors(u, v, tu, tv), time=1.5)
+    want_loss, want_g = net_cpu.loss_and_grads(w, u, v, tu, tv, time=1.5)
     assert abs(loss - want_loss) <= 1e-5 * want_loss
     # BF16 operands, FP32 accumulation on both sides: the gradient as a whole to 1 %, its large entries to 3 %.
     assert np.linalg.norm(g - want_g) <= 1e-2 * np.linalg.norm(want_g)
@@ -68,7 +68,7 @@ def test_loss_and_gradients_match_the_oracle(cuda):
     assert np.all(np.abs(g[big] - want_g[big]) <= 3e-2 * np.abs(want_g[big]))
     assert np.all(g[net_cpu.pad_mask()] == 0.0)
     # Deterministic: the CTAs' partial sums are added in a fixed order.
-    loss2, g2 = c.grads(*tensors(u, v, tu, tv))
+    loss2, g2 = c.grads(*tensors(u, v, tu, tv), time=1.5)
     assert loss2 == loss and np.array_equal(g2.view(np.uint32), g.view(np.uint32))
     c.close()
 
@@ -111,38 +111,14 @@ def test_the_guard_keeps_the_plain_step_when_a_cell_leaves_the_range(cuda):
 def test_trained_correction_beats_the_coarse_plain_method(cuda):
     """FitzHugh-Nagumo, fine 128 x 128 as the judge: the coarse 32 x 32 plain solve with the trained correction ends
     closer to the fine solution (averaged onto 32 x 32) than the coarse plain solve alone, on seeds it did not see."""
-    import torch
-    from fieldcuda.learned import Corrector, PlainFHN, block_mean, fhn_initial, init_weights
+    from fieldcuda.learned import Corrector, PlainFHN, fine_frames, init_weights, train_correction
     text = law()
     frames = 20
-
-    def fine_frames(seeds):
-        u0, v0 = fhn_initial(seeds, 128)
-        fine = PlainFHN(text, 128, len(seeds))
-        fine.set(u0, v0)
-        out = []
-        for t in range(frames + 1):
-            if t:
-                fine.step()
-            u, v = fine.get()
-            out.append((torch.nn.functional.avg_pool2d(u[:, None], 4)[:, 0].contiguous(),
-                        torch.nn.functional.avg_pool2d(v[:, None], 4)[:, 0].contiguous()))
-        fine.close()
-        return out
-
-    train = fine_frames(list(range(100, 124)))
-    test = fine_frames(list(range(900, 906)))
-    coarse = PlainFHN(text, 32, 24)
+    train = fine_frames(text, list(range(100, 124)), frames)
+    test = fine_frames(text, list(range(900, 906)), frames)
     c = Corrector(init_weights(7))
-    pairs = []
-    for t in range(frames):
-        coarse.set(*train[t])
-        coarse.step()
-        pairs.append((*coarse.get(), *train[t + 1]))
-    coarse.close()
-    for it in range(600):
-        u, v, tu, tv = pairs[it % frames]
-        c.train_step(u, v, tu, tv, 2e-3)
+    best, plain_train = train_correction(c, text, train, iters=600, rounds=1)
+    assert best < plain_train
 
     def rollout(correct):
         s = PlainFHN(text, 32, 6)
@@ -153,7 +129,7 @@ def test_trained_correction_beats_the_coarse_plain_method(cuda):
             s.step()
             u, v = s.get()
             if correct:
-                c.apply(u, v, -1000.0, 1000.0)
+                c.apply(u, v, -1000.0, 1000.0, time=(t + 1) * 0.05 * c.time_scale)
             tu, tv = test[t + 1]
             err += float(((u - tu) ** 2 + (v - tv) ** 2).mean())
         s.close()
