@@ -657,6 +657,50 @@ def run_ours(args, world, rank, local):
     }))
 
 
+def profile_case(name):
+    """Small cases of the kernels the profiles under profiles/ summarise, for ncu (one GPU; a few launches):
+    heston      36 options on 512 x 256, 16 Douglas steps, split (16, 4, 512): the cluster kernel;
+    corrector   3 training steps, one gradient and one guarded apply on 256 x 32 x 32 cells: the tcgen05 kernels;
+    multifield  the 43-term law on 128^3, 3 steps: its generated passes."""
+    import numpy as np
+    import torch
+    if name == "heston":
+        from fieldcuda.heston import HestonBatch, sample_options
+        with HestonBatch(sample_options(36, 1, sizes=((512, 256),)), 16, 0) as b:
+            b.set_split(16, 4, 512)
+            b.run()
+            b.prices()
+            print(json.dumps({"case": name, "ms": b.time(False), "layout": b.layout()}))
+    elif name == "corrector":
+        from fieldcuda.learned import Corrector, init_weights
+        rng = np.random.default_rng(0)
+        u, v, tu, tv = (torch.tensor(rng.normal(size=(256, 32, 32)).astype(np.float32), device="cuda") for _ in range(4))
+        c = Corrector(init_weights(1))
+        for _ in range(3):
+            c.train_step(u, v, tu, tv, 1e-3)
+        loss, _ = c.grads(u, v, tu, tv)
+        c.apply(u, v)
+        torch.cuda.synchronize()
+        c.close()
+        print(json.dumps({"case": name, "loss": loss}))
+    elif name == "multifield":
+        from fieldcuda.solver import Solver
+        from fieldcuda.workloads import multifield_law
+        text, _ = multifield_law(0)
+        n = 128
+        s = Solver(text, n, n, n, 1.0 / n, "multifield43.law")
+        rng = np.random.default_rng(43)
+        for i in range(6):
+            s.set_field(f"f{i}", rng.uniform(-1, 1, (n, n, n)).astype(np.float32))
+        for _ in range(3):
+            s.step(0.1 / (n * n))
+        s.sync()
+        print(json.dumps({"case": name, "violations": len(s.violations())}))
+        s.close()
+    else:
+        raise SystemExit(f"no profile case {name!r}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -669,7 +713,11 @@ def main():
     ap.add_argument("--no-multifield", action="store_true", help="skip the 43-term multi-field law section")
     ap.add_argument("--no-calibration", action="store_true", help="skip the adjoint calibration section")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-correction section")
+    ap.add_argument("--profile-case", default="", help="run one small case for ncu (heston, corrector, multifield) and exit")
     args = ap.parse_args()
+    if args.profile_case:
+        profile_case(args.profile_case)
+        return
     world, rank, local = init_dist()
     try:
         if args.impl == "reference":

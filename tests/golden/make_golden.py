@@ -90,6 +90,15 @@ def cases():
     rngt = np.random.default_rng(7)
     out.append(dict(name="ops_transposed", law="ops_transposed.law", shape=n, h=0.5, dt=0.01, steps=3,
                     fields={"a": rngt.uniform(-1, 1, n).astype(np.float32), "b": rngt.uniform(-1, 1, n).astype(np.float32)}))
+    # Lattices at least one slab tile (128 cells) wide: the generated TMA slab passes rather than the plain ones.
+    n = (5, 9, 136)
+    rngw = np.random.default_rng(11)
+    out.append(dict(name="ops_stencil_wide", law="ops_stencil.law", shape=n, h=0.5, dt=0.01, steps=3,
+                    fields={"a": rngw.uniform(-1, 1, n).astype(np.float32),
+                            "k": rngw.uniform(0.5, 2.0, n).astype(np.float32)}))
+    n = (4, 6, 128)
+    out.append(dict(name="multifield43_wide", law="multifield43.law", shape=n, h=1.0 / 128, dt=0.1 * (1.0 / 128) ** 2, steps=2,
+                    fields={f"f{i}": rngw.uniform(-1, 1, n).astype(np.float32) for i in range(6)}))
     n = (12, 16, 20)
     rngm = np.random.default_rng(43)
     out.append(dict(name="multifield43", law="multifield43.law", shape=n, h=1.0 / 20, dt=0.1 * (1.0 / 20) ** 2, steps=3,

@@ -68,7 +68,7 @@ def test_engine_heat_bit_identical_to_handwritten_kernel(cuda):
     from fieldcuda import kernels
     from fieldcuda.solver import Solver
     from oracle import heat as oh
-    for n in (64, 96):
+    for n in (64, 96, 128, 160):   # the first two take the plain pass, the last two the TMA slab pass
         h = 1.0 / n
         dt = 0.4 * h * h / 6.0
         T0 = oh.gaussian_blobs(n, h, seed=3)
