@@ -659,6 +659,7 @@ def run_ours(args, world, rank, local):
 
 def profile_case(name):
     """Small cases of the kernels the profiles under profiles/ summarise, for ncu (one GPU; a few launches):
+    heat        the heat law on 384^3 (inputs larger than L2), 3 steps: the generated gather;
     heston      36 options on 512 x 256, 16 Douglas steps, split (16, 4, 512): the cluster kernel;
     corrector   3 training steps, one gradient and one guarded apply on 256 x 32 x 32 cells: the tcgen05 kernels;
     multifield  the 43-term law on 128^3, 3 steps: its generated passes."""
@@ -683,6 +684,18 @@ def profile_case(name):
         torch.cuda.synchronize()
         c.close()
         print(json.dumps({"case": name, "loss": loss}))
+    elif name == "heat":
+        from fieldcuda.solver import Solver
+        from oracle import heat as oh
+        n = 384
+        h = 1.0 / n
+        s = Solver(HEAT_LAW, n, n, n, h, "heat.law")
+        s.set_field("T", oh.gaussian_blobs(n, h, seed=0))
+        for _ in range(3):
+            s.step(0.4 * h * h / 6.0)
+        s.sync()
+        print(json.dumps({"case": name, "violations": len(s.violations())}))
+        s.close()
     elif name == "multifield":
         from fieldcuda.solver import Solver
         from fieldcuda.workloads import multifield_law

@@ -189,7 +189,8 @@ CUfunction Engine::function(const std::string& name, unsigned smem, std::string&
     if (found != functions_.end()) return found->second;
     CUfunction fn = nullptr;
     if (!cu_ok(driver().moduleGetFunction(&fn, module_, name.c_str()), ("kernel " + name).c_str(), why)) return nullptr;
-    if (smem > 48 * 1024 &&
+    // The default cap (48 KB) counts static and dynamic shared memory together: any dynamic size gets its attribute.
+    if (smem > 0 &&
         !cu_ok(driver().funcSetAttribute(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, static_cast<int>(smem)), "smem attribute", why)) {
         return nullptr;
     }
