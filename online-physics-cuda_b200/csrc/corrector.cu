@@ -47,12 +47,23 @@ constexpr int kWeights = kW1 + kW2 + kW3;
 // 128 cells x 16 bytes; then the weights, dY (2 groups), dZ2 and dZ1 (8 each).
 constexpr unsigned kGroup = kTile * 16;
 constexpr unsigned kX0 = 0, kH1 = 4 * kGroup, kH2 = 14 * kGroup, kStack = 30 * kGroup;
-constexpr unsigned kWB1 = kStack, kWB2 = kWB1 + kW1 * 2, kWB3 = kWB2 + kW2 * 2, kWEnd = kWB3 + kW3 * 2;
-constexpr unsigned kDY = kWEnd, kDZ2 = kDY + 2 * kGroup, kDZ1 = kDZ2 + 8 * kGroup, kBar = kDZ1 + 8 * kGroup;
-constexpr unsigned kSmem = kBar + 64;
 // Tensor memory columns (FP32): Z1 | Z2 | Y | dH2 | dH1 | dW1 | dW2 | dW3.
-constexpr unsigned kTZ1 = 0, kTZ2 = 64, kTY = 128, kTDH2 = 144, kTDH1 = 224, kTDW1 = 304, kTDW2 = 368, kTDW3 = 432;
-constexpr unsigned kTCols = 512;
+constexpr unsigned kTZ1 = 0, kTZ2 = 64, kTDH2 = 144, kTDH1 = 224, kTDW1 = 304, kTDW2 = 368, kTDW3 = 432;
+
+// The two layouts. Training keeps the spare groups after H2 (the weight-gradient MMAs read 128 feature rows from X0, H1
+// or H2), dY, dZ2, dZ1 and 512 tensor-memory columns: one CTA an SM. Inference needs X0 | H1 | H2 and the weights
+// (65 KB) and 128 columns (Y reuses Z1's, consumed by then): three CTAs an SM.
+template <bool TRAIN>
+struct Layout {
+    static constexpr unsigned WB1 = TRAIN ? kStack : 24 * kGroup;
+    static constexpr unsigned WB2 = WB1 + kW1 * 2, WB3 = WB2 + kW2 * 2, WEnd = WB3 + kW3 * 2;
+    static constexpr unsigned DY = WEnd, DZ2 = DY + 2 * kGroup, DZ1 = DZ2 + 8 * kGroup;
+    static constexpr unsigned BAR = TRAIN ? DZ1 + 8 * kGroup : WEnd;
+    static constexpr unsigned SMEM = BAR + 64;
+    static constexpr unsigned TY = TRAIN ? 128u : 0u;
+    static constexpr unsigned TCOLS = TRAIN ? 512u : 128u;
+    static constexpr int PER_SM = TRAIN ? 1 : 3;
+};
 constexpr unsigned kWaitLimit = 1u << 22;
 
 struct CorrArgs {
@@ -190,17 +201,18 @@ __device__ __forceinline__ void relu_back(unsigned tdh, unsigned tz, unsigned ch
 }
 
 template <bool TRAIN>
-__global__ void __launch_bounds__(kThreadsC, 1) corr_kernel(const CorrArgs a)
+__global__ void __launch_bounds__(kThreadsC, Layout<TRAIN>::PER_SM) corr_kernel(const CorrArgs a)
 {
+    using L = Layout<TRAIN>;
     extern __shared__ __align__(1024) unsigned char sm[];
-    fe_u64* bar = reinterpret_cast<fe_u64*>(sm + kBar);
-    unsigned* tslot = reinterpret_cast<unsigned*>(sm + kBar + 16);
+    fe_u64* bar = reinterpret_cast<fe_u64*>(sm + L::BAR);
+    unsigned* tslot = reinterpret_cast<unsigned*>(sm + L::BAR + 16);
     const int t = threadIdx.x;
     const int warp = t >> 5;
     // Weights into shared memory (already in their core layouts), the mbarrier, tensor memory.
     {
         const uint4* src = reinterpret_cast<const uint4*>(a.w);
-        uint4* dst = reinterpret_cast<uint4*>(sm + kWB1);
+        uint4* dst = reinterpret_cast<uint4*>(sm + L::WB1);
         for (int i = t; i < kWeights * 2 / 16; i += kThreadsC) dst[i] = src[i];
     }
     if (t == 0) {
@@ -208,7 +220,7 @@ __global__ void __launch_bounds__(kThreadsC, 1) corr_kernel(const CorrArgs a)
         fe_fence_mbar_init();
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(fe_smem(tslot)), "r"(kTCols) : "memory");
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(fe_smem(tslot)), "r"(L::TCOLS) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     fe_fence_proxy_async();
@@ -260,7 +272,7 @@ __global__ void __launch_bounds__(kThreadsC, 1) corr_kernel(const CorrArgs a)
         if (t == 0) {
             tc_after();
             for (int k = 0; k < 2; ++k) {
-                mma(tbase + kTZ1, sdesc(s0 + kX0 + k * 2 * kGroup, kGroup, 128), sdesc(s0 + kWB1 + k * 2 * 128, 128, (32 / 8) * 128),
+                mma(tbase + kTZ1, sdesc(s0 + kX0 + k * 2 * kGroup, kGroup, 128), sdesc(s0 + L::WB1 + k * 2 * 128, 128, (32 / 8) * 128),
                     idesc(128, 64, false, true), k > 0);
             }
             mma_commit(bar);
@@ -272,7 +284,7 @@ __global__ void __launch_bounds__(kThreadsC, 1) corr_kernel(const CorrArgs a)
         if (t == 0) {
             tc_after();
             for (int k = 0; k < 5; ++k) {
-                mma(tbase + kTZ2, sdesc(s0 + kH1 + k * 2 * kGroup, kGroup, 128), sdesc(s0 + kWB2 + k * 2 * 128, 128, (80 / 8) * 128),
+                mma(tbase + kTZ2, sdesc(s0 + kH1 + k * 2 * kGroup, kGroup, 128), sdesc(s0 + L::WB2 + k * 2 * 128, 128, (80 / 8) * 128),
                     idesc(128, 64, false, true), k > 0);
             }
             mma_commit(bar);
@@ -284,14 +296,14 @@ __global__ void __launch_bounds__(kThreadsC, 1) corr_kernel(const CorrArgs a)
         if (t == 0) {
             tc_after();
             for (int k = 0; k < 5; ++k) {
-                mma(tbase + kTY, sdesc(s0 + kH2 + k * 2 * kGroup, kGroup, 128), sdesc(s0 + kWB3 + k * 2 * 128, 128, (80 / 8) * 128),
+                mma(tbase + L::TY, sdesc(s0 + kH2 + k * 2 * kGroup, kGroup, 128), sdesc(s0 + L::WB3 + k * 2 * 128, 128, (80 / 8) * 128),
                     idesc(128, 16, false, true), k > 0);
             }
             mma_commit(bar);
         }
         if (!(ok = mma_wait(bar, phase, a.err))) break;
         float y[16];
-        tld16(lane_base + kTY, y);
+        tld16(lane_base + L::TY, y);
         tld_wait();
         if constexpr (!TRAIN) {
             if (valid) {
@@ -314,42 +326,42 @@ __global__ void __launch_bounds__(kThreadsC, 1) corr_kernel(const CorrArgs a)
             dy[1] = vc + y[1] - a.tv[cell];
             loss += 0.5 * (static_cast<double>(dy[0]) * dy[0] + static_cast<double>(dy[1]) * dy[1]);
         }
-        put8(sm + kDY, t, 0, kTile, dy);
-        put8(sm + kDY, t, 8, kTile, dy + 8);
+        put8(sm + L::DY, t, 0, kTile, dy);
+        put8(sm + L::DY, t, 8, kTile, dy + 8);
         hand_over();
         if (t == 0) {
             tc_after();
-            mma(tbase + kTDH2, sdesc(s0 + kDY, kGroup, 128), sdesc(s0 + kWB3, (80 / 8) * 128, 128), idesc(128, 80, false, false), 0);
+            mma(tbase + kTDH2, sdesc(s0 + L::DY, kGroup, 128), sdesc(s0 + L::WB3, (80 / 8) * 128, 128), idesc(128, 80, false, false), 0);
             for (int k = 0; k < 8; ++k) {
-                mma(tbase + kTDW3, sdesc(s0 + kH2 + k * 256, 128, kGroup), sdesc(s0 + kDY + k * 256, 128, kGroup), idesc(128, 16, true, true),
+                mma(tbase + kTDW3, sdesc(s0 + kH2 + k * 256, 128, kGroup), sdesc(s0 + L::DY + k * 256, 128, kGroup), idesc(128, 16, true, true),
                     done > 0 || k > 0);
             }
             mma_commit(bar);
         }
         if (!(ok = mma_wait(bar, phase, a.err))) break;
         // 5. dZ2 = dH2 (Z2 > 0); dH1 = dZ2 W2^T and dW2 += H1^T dZ2.
-        relu_back(lane_base + kTDH2, lane_base + kTZ2, sm, kDZ2, t, valid);
+        relu_back(lane_base + kTDH2, lane_base + kTZ2, sm, L::DZ2, t, valid);
         hand_over();
         if (t == 0) {
             tc_after();
             for (int k = 0; k < 4; ++k) {
-                mma(tbase + kTDH1, sdesc(s0 + kDZ2 + k * 2 * kGroup, kGroup, 128), sdesc(s0 + kWB2 + k * 2 * (80 / 8) * 128, (80 / 8) * 128, 128),
+                mma(tbase + kTDH1, sdesc(s0 + L::DZ2 + k * 2 * kGroup, kGroup, 128), sdesc(s0 + L::WB2 + k * 2 * (80 / 8) * 128, (80 / 8) * 128, 128),
                     idesc(128, 80, false, false), k > 0);
             }
             for (int k = 0; k < 8; ++k) {
-                mma(tbase + kTDW2, sdesc(s0 + kH1 + k * 256, 128, kGroup), sdesc(s0 + kDZ2 + k * 256, 128, kGroup), idesc(128, 64, true, true),
+                mma(tbase + kTDW2, sdesc(s0 + kH1 + k * 256, 128, kGroup), sdesc(s0 + L::DZ2 + k * 256, 128, kGroup), idesc(128, 64, true, true),
                     done > 0 || k > 0);
             }
             mma_commit(bar);
         }
         if (!(ok = mma_wait(bar, phase, a.err))) break;
         // 6. dZ1 = dH1 (Z1 > 0); dW1 += X0^T dZ1.
-        relu_back(lane_base + kTDH1, lane_base + kTZ1, sm, kDZ1, t, valid);
+        relu_back(lane_base + kTDH1, lane_base + kTZ1, sm, L::DZ1, t, valid);
         hand_over();
         if (t == 0) {
             tc_after();
             for (int k = 0; k < 8; ++k) {
-                mma(tbase + kTDW1, sdesc(s0 + kX0 + k * 256, 128, kGroup), sdesc(s0 + kDZ1 + k * 256, 128, kGroup), idesc(128, 64, true, true),
+                mma(tbase + kTDW1, sdesc(s0 + kX0 + k * 256, 128, kGroup), sdesc(s0 + L::DZ1 + k * 256, 128, kGroup), idesc(128, 64, true, true),
                     done > 0 || k > 0);
             }
             mma_commit(bar);
@@ -397,7 +409,7 @@ __global__ void __launch_bounds__(kThreadsC, 1) corr_kernel(const CorrArgs a)
     __syncthreads();
     if (warp == 0) {
         tc_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(L::TCOLS) : "memory");
     }
 }
 
@@ -507,9 +519,9 @@ int run_grads(fe_corrector* c, const float* u, const float* v, const float* tu, 
     a.tv = tv;
     a.time = time;
     const long long tiles = (a.cells + fe::kTile - 1) / fe::kTile;
-    const int grid = static_cast<int>(std::min<long long>(tiles, c->ctas));
+    const int grid = static_cast<int>(std::min<long long>(tiles, static_cast<long long>(c->ctas) * fe::Layout<true>::PER_SM));
     if (!fe::cuda_ok(cudaMemsetAsync(c->err, 0, 4 * sizeof(unsigned), s), "reset", why)) return fe::fail(FE_ECUDA, why);
-    fe::corr_kernel<true><<<grid, fe::kThreadsC, fe::kSmem, s>>>(a);
+    fe::corr_kernel<true><<<grid, fe::kThreadsC, fe::Layout<true>::SMEM, s>>>(a);
     ++c->adam_t;
     const float b1t = lr > 0.f ? 1.f - std::pow(0.9f, static_cast<float>(c->adam_t)) : 1.f;
     const float b2t = lr > 0.f ? 1.f - std::pow(0.999f, static_cast<float>(c->adam_t)) : 1.f;
@@ -548,8 +560,10 @@ int fe_corr_create(fe_corrector** out)
     if (!fe::device_ready(why)) return fe::fail(FE_ENODEV, why);
     auto* c = new fe_corrector();
     c->ctas = fe::sm_count();
-    bool ok = fe::cuda_ok(cudaFuncSetAttribute(fe::corr_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(fe::kSmem)), "smem", why) &&
-        fe::cuda_ok(cudaFuncSetAttribute(fe::corr_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(fe::kSmem)), "smem", why) &&
+    bool ok = fe::cuda_ok(cudaFuncSetAttribute(fe::corr_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(fe::Layout<true>::SMEM)), "smem", why) &&
+        fe::cuda_ok(cudaFuncSetAttribute(fe::corr_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                        static_cast<int>(fe::Layout<false>::SMEM)), "smem", why) &&
         fe::cuda_ok(cudaMalloc(&c->w, sizeof(float) * fe::kWeights), "w", why) && fe::cuda_ok(cudaMalloc(&c->m, sizeof(float) * fe::kWeights), "m", why) &&
         fe::cuda_ok(cudaMalloc(&c->v, sizeof(float) * fe::kWeights), "v", why) &&
         fe::cuda_ok(cudaMalloc(&c->wb, sizeof(unsigned short) * fe::kWeights), "wb", why) &&
@@ -635,9 +649,9 @@ int fe_corr_apply(fe_corrector* c, float* u, float* v, int nx, int ny, int nz, f
     a.hi = hi;
     a.time = time;
     const long long tiles = (a.cells + fe::kTile - 1) / fe::kTile;
-    const int grid = static_cast<int>(std::min<long long>(tiles, c->ctas));
+    const int grid = static_cast<int>(std::min<long long>(tiles, static_cast<long long>(c->ctas) * fe::Layout<false>::PER_SM));
     if (!fe::cuda_ok(cudaMemsetAsync(c->err, 0, 4 * sizeof(unsigned), s), "reset", why)) return fe::fail(FE_ECUDA, why);
-    fe::corr_kernel<false><<<grid, fe::kThreadsC, fe::kSmem, s>>>(a);
+    fe::corr_kernel<false><<<grid, fe::kThreadsC, fe::Layout<false>::SMEM, s>>>(a);
     fe::corr_commit<<<std::max(1, std::min(1024, static_cast<int>((a.cells + 255) / 256))), 256, 0, s>>>(c->ou, c->ov, u, v, a.cells, c->err,
         c->err + 2);
     if (!fe::cuda_ok(cudaGetLastError(), "corrector launch", why)) return fe::fail(FE_ECUDA, why);
