@@ -398,11 +398,12 @@ struct FeSlabCtx {
     }
 };
 
-// For passes whose x edge the halo can carry (P::XFILL): after plane j lands, the staged columns past the lattice's x
+// For passes whose x edge the halo can carry (P::XFILL): after a plane lands in ring stage `stage`, the staged columns
+// past the lattice's x
 // edge get the edge cell's value, what a clamped read returns there. Only the CTAs at an x edge do anything; one row a
 // thread.
 template <class P>
-__device__ __forceinline__ void fe_fill_x_edges(float* sm, int j, int x0)
+__device__ __forceinline__ void fe_fill_x_edges(float* sm, int stage, int x0)
 {
     if (!P::XFILL) return;
     const bool left = x0 == 0;
@@ -415,7 +416,7 @@ __device__ __forceinline__ void fe_fill_x_edges(float* sm, int j, int x0)
         if (ax == 0) continue;
         const int rows = P::W * P::R + 2 * P::ry(k);
         const int px = P::px(k);
-        float* plane = sm + P::base(k) + (j % P::NST) * P::pl(k);
+        float* plane = sm + P::base(k) + stage * P::pl(k);
         for (int row = threadIdx.x; row < rows; row += blockDim.x) {
             float* r = plane + row * px;
             if (left) {
@@ -467,7 +468,6 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
     extern __shared__ __align__(128) float fe_sm[];
     __shared__ __align__(8) fe_u64 bar[P::NST];
     __shared__ double scratch[4 * P::W];
-    __shared__ int failed;
     static_assert(P::NST >= 2 * P::RZ + 2, "the ring holds 2 RZ + 1 planes and the one being fetched");
     const int x0 = blockIdx.x * 128;
     const int y0 = blockIdx.y * (P::W * P::R);
@@ -478,17 +478,17 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
     const int nplanes = zhi - zlo + 1;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
+    // Plane j of the chunk (lattice plane zlo + j) lands in ring stage j % NST, in phase (j / NST) & 1 of its barrier.
     auto issue = [&](int j) {
-        fe_mbar_expect_tx(&bar[j % P::NST], P::BYTES);
+        const int st = j % P::NST;
+        fe_mbar_expect_tx(&bar[st], P::BYTES);
 #pragma unroll
         for (int k = 0; k < P::NSRC; ++k) {
-            fe_tma_load_3d(fe_sm + P::base(k) + (j % P::NST) * P::pl(k), &a.map[k], &bar[j % P::NST], x0 - P::ax(k),
-                y0 - P::ry(k), zlo + j);
+            fe_tma_load_3d(fe_sm + P::base(k) + st * P::pl(k), &a.map[k], &bar[st], x0 - P::ax(k), y0 - P::ry(k), zlo + j);
         }
     };
     int issued = 0;
     if (threadIdx.x == 0) {
-        failed = 0;
         for (int s = 0; s < P::NST; ++s) fe_mbar_init(&bar[s], 1);
         fe_fence_mbar_init();
         issued = min(P::NST, nplanes);
@@ -498,22 +498,48 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
     FeAcc acc[P::NOUT];
 #pragma unroll
     for (int j = 0; j < P::NOUT; ++j) fe_acc_init(acc[j]);
+    // Every thread waits (bounded) for the planes a z needs, and evens the x edge of each plane that landed (XFILL);
+    // the barrier that follows makes both visible and, OR-ing the outcomes, the decision to go on uniform. The next
+    // plane to wait for is tracked by its stage and phase, stepped rather than divided.
     int waited = 0;
-    // Every thread waits (bounded) for the planes a z needs, and evens the x edge of each plane that landed (XFILL); the
-    // barrier that follows makes both visible and the outcome uniform.
+    int wst = 0;
+    unsigned wpar = 0u;
+    bool ok = true;
+    const bool edge = P::XFILL && (x0 == 0 || x0 + 128 >= P::NX);
     auto wait_upto = [&](int j) {
         while (waited <= j) {
-            if (!fe_mbar_wait(&bar[waited % P::NST], static_cast<unsigned>((waited / P::NST) & 1), 1u << 20)) failed = 1;
-            else fe_fill_x_edges<P>(fe_sm, waited, x0);
+            if (!fe_mbar_wait(&bar[wst], wpar, 1u << 20)) ok = false;
+            else if (edge) fe_fill_x_edges<P>(fe_sm, wst, x0);
             ++waited;
+            if (++wst == P::NST) {
+                wst = 0;
+                wpar ^= 1u;
+            }
         }
     };
     if (zb < ze) wait_upto(min(zb + P::RZ, P::NZ - 1) - zlo);
-    __syncthreads();
+    bool failed = __syncthreads_or(ok ? 0 : 1) != 0;
     const int x = x0 + 4 * lane;
     // With the x edge carried by the halo, whether a row's cells are interior depends only on the row and the plane, so
-    // a warp takes one path.
+    // a warp takes one path. Which of this warp's rows lie in the lattice, and which have their whole y reach inside
+    // it, are fixed for the pass.
     const bool xin = P::XFILL || (x - P::RXT >= 0 && x + 3 + P::RXT < P::NX);
+    constexpr bool ragged = (P::NY % (P::W * P::R)) != 0 || (P::NX % 128) != 0;
+    unsigned live = 0u;
+    unsigned yin = 0u;
+#pragma unroll
+    for (int r = 0; r < P::R; ++r) {
+        const int y = y0 + warp * P::R + r;
+        if (y < P::NY && x < P::NX) live |= 1u << r;
+        if (y - P::RYT >= 0 && y + P::RYT < P::NY) yin |= 1u << r;
+    }
+    const bool totals_before = (a.flags & FE_PASS_BEFORE) != 0;
+    const bool totals_after = (a.flags & FE_PASS_AFTER) != 0;
+    const bool range = (a.flags & FE_PASS_RANGE) != 0;
+    const fe_u64 row0 = static_cast<fe_u64>(P::NX) * static_cast<fe_u64>(y0 + warp * P::R) + static_cast<fe_u64>(x);
+    // The ring stage of plane z, stepped with z; planes whose z reach stays in the lattice take their neighbours'
+    // stages from it, the clamped ones at the lattice's z ends recompute them.
+    int sz = zb - zlo;
     for (int z = zb; z < ze && !failed; ++z) {
         FeSlabCtx<P> c;
         c.sm = fe_sm;
@@ -521,46 +547,56 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         c.y0 = y0;
         c.z = z;
         c.dt = a.dt;
+        if (z - P::RZ >= 0 && z + P::RZ < P::NZ) {
 #pragma unroll
-        for (int d = -P::RZ; d <= P::RZ; ++d) c.slots[d + P::RZ] = (min(max(z + d, 0), P::NZ - 1) - zlo) % P::NST;
-        const bool zin = z - P::RZT >= 0 && z + P::RZT < P::NZ;
+            for (int d = -P::RZ; d <= P::RZ; ++d) {
+                int st = sz + d;
+                if (d < 0 && st < 0) st += P::NST;
+                if (d > 0 && st >= P::NST) st -= P::NST;
+                c.slots[d + P::RZ] = st;
+            }
+        } else {
+#pragma unroll
+            for (int d = -P::RZ; d <= P::RZ; ++d) c.slots[d + P::RZ] = (min(max(z + d, 0), P::NZ - 1) - zlo) % P::NST;
+        }
+        const bool plane_in = xin && z - P::RZT >= 0 && z + P::RZT < P::NZ;
+        const fe_u64 plane0 = static_cast<fe_u64>(P::NX) * static_cast<fe_u64>(P::NY) * static_cast<fe_u64>(z) + row0;
 #pragma unroll
         for (int r = 0; r < P::R; ++r) {
+            if (ragged && !((live >> r) & 1u)) continue;
             const int y = y0 + warp * P::R + r;
-            if (y >= P::NY || x >= P::NX) continue;
             float o[4][P::NOUT];
             float b[4][P::NOUT];
             // Four cells whose whole reach is inside the lattice take the clamp-free code; the rest the clamped one.
-            const bool in = zin && xin && y - P::RYT >= 0 && y + P::RYT < P::NY;
-            if (in) {
+            if (plane_in && ((yin >> r) & 1u)) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) P::template cell<true>(c, x + q, y, z, o[q], b[q]);
             } else {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) P::template cell<false>(c, x + q, y, z, o[q], b[q]);
             }
-            const fe_u64 at = static_cast<fe_u64>(x) + static_cast<fe_u64>(P::NX) * (static_cast<fe_u64>(y) + static_cast<fe_u64>(P::NY) * z);
+            const fe_u64 at = plane0 + static_cast<fe_u64>(r) * P::NX;
 #pragma unroll
             for (int j = 0; j < P::NOUT; ++j) {
                 *reinterpret_cast<float4*>(a.out[j] + at) = make_float4(o[0][j], o[1][j], o[2][j], o[3][j]);
                 if (P::checked(j) && a.rec[j] != nullptr) {
                     const float bb[4] = {b[0][j], b[1][j], b[2][j], b[3][j]};
                     const float oo[4] = {o[0][j], o[1][j], o[2][j], o[3][j]};
-                    fe_acc_row4(acc[j], bb, oo, a.lo[j], a.hi[j], static_cast<unsigned>(at), (a.flags & FE_PASS_BEFORE) != 0,
-                        (a.flags & FE_PASS_AFTER) != 0, (a.flags & FE_PASS_RANGE) != 0);
+                    fe_acc_row4(acc[j], bb, oo, a.lo[j], a.hi[j], static_cast<unsigned>(at), totals_before, totals_after, range);
                 }
             }
         }
 #pragma unroll
         for (int j = 0; j < P::NOUT; ++j) fe_acc_flush(acc[j]);
         if (z + 1 < ze) wait_upto(min(z + 1 + P::RZ, P::NZ - 1) - zlo);
-        __syncthreads();
+        failed = __syncthreads_or(ok ? 0 : 1) != 0;
         const int release = z - P::RZ - zlo;
         if (threadIdx.x == 0 && !failed && release >= 0 && release + P::NST < nplanes) {
             fe_fence_proxy_async();
             issue(release + P::NST);
             issued = release + P::NST + 1;
         }
+        if (++sz == P::NST) sz = 0;
     }
     if (failed) {
         if (threadIdx.x == 0) {
