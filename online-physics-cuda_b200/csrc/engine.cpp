@@ -114,6 +114,7 @@ bool Engine::create(const std::vector<law::Source>& sources, int nx, int ny, int
     }
     bounds_.assign(fields, Bounds{});
     zero_.assign(fields, 0);
+    carry_.assign(fields, Carry{});
     for (std::size_t f = 0; f < fields; ++f) {
         const float init = static_cast<float>(law_.fields[f].init);
         if (!cuda_ok(launch_fill(now_[f], cells_, init, sms_, stream_), "fill", why)) return false;
@@ -215,7 +216,7 @@ int Engine::zchunk_for(const gen::Launch& L, bool slab) const
     return std::max(1, zchunk);
 }
 
-bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* recs, std::string& why)
+bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* recs, std::string& why, const FeCheck* const* carry)
 {
     FePassArgs a;
     std::memset(&a, 0, sizeof(a));
@@ -236,6 +237,9 @@ bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* r
         }
         const int f = j < L.checked_fields.size() ? L.checked_fields[j] : -1;
         a.rec[j] = (recs != nullptr && f >= 0) ? recs[j] : nullptr;
+        a.carry[j] = (a.rec[j] != nullptr && carry != nullptr) ? carry[j] : nullptr;
+        // Whatever held the totals of this field's contents no longer does; the caller renews it after a checked gather.
+        if (L.outs[j].kind != gen::Buf::Slot && L.outs[j].id >= 0) carry_[static_cast<std::size_t>(L.outs[j].id)] = Carry{};
         a.lo[j] = f >= 0 ? static_cast<float>(law_.fields[static_cast<std::size_t>(f)].lo) : -3.0e38f;
         a.hi[j] = f >= 0 ? static_cast<float>(law_.fields[static_cast<std::size_t>(f)].hi) : 3.0e38f;
     }
@@ -292,6 +296,16 @@ bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* r
         ("launch " + name).c_str(), why);
 }
 
+bool Engine::conserved_by(int term, int field) const
+{
+    for (const std::vector<int>& group : law_.terms[static_cast<std::size_t>(term)].conserves) {
+        for (const int f : group) {
+            if (f == field) return true;
+        }
+    }
+    return false;
+}
+
 bool Engine::set_param(int id, double value)
 {
     if (id < 0 || static_cast<std::size_t>(id) >= param_host_.size()) return false;
@@ -330,6 +344,7 @@ bool Engine::upload(int field, const void* src, bool device, std::string& why)
     }
     bounds_[static_cast<std::size_t>(field)] = b;
     zero_[static_cast<std::size_t>(field)] = (b.lo == 0.0 && b.hi == 0.0) ? 1 : 0;
+    carry_[static_cast<std::size_t>(field)] = Carry{};
     return true;
 }
 
@@ -338,6 +353,7 @@ void Engine::mark_edited(int field)
     if (field < 0 || static_cast<std::size_t>(field) >= now_.size()) return;
     bounds_[static_cast<std::size_t>(field)] = Bounds{};
     zero_[static_cast<std::size_t>(field)] = 0;
+    carry_[static_cast<std::size_t>(field)] = Carry{};
 }
 
 bool Engine::fetch(int field, void* dst, bool device, std::string& why)
@@ -587,22 +603,42 @@ bool Engine::run_program(int index, const ir::Program& p, const gen::ProgramPlan
     substeps_[static_cast<std::size_t>(index)] = count;
     const float sub_dt = static_cast<float>(dt / count);
     FeCheck* recs[FE_MAX_OUT] = {};
+    const FeCheck* carried[FE_MAX_OUT] = {};
+    int rec_index[FE_MAX_OUT] = {};
     if (check) {
         for (std::size_t j = 0; j < pp.gather.outs.size(); ++j) {
             const int r = static_cast<int>(pending.refs.size());
+            const int f = pp.gather.checked_fields[j];
+            rec_index[j] = r;
             recs[j] = records_ + static_cast<std::size_t>(pending.ring) * records_per_step_ + r;
-            pending.refs.push_back(RecordRef{index, pp.gather.checked_fields[j], r, count, true});
+            pending.refs.push_back(RecordRef{index, f, r, count, true});
+            if (f < 0) continue;
+            // The totals before the term: those after the checked pass that last wrote the field (still in the ring),
+            // else, for a conserved field, summed now.
+            const Carry& c = carry_[static_cast<std::size_t>(f)];
+            if (c.step >= 0 && steps_ - c.step < ring_ - 2) {
+                carried[j] = records_ + static_cast<std::size_t>(c.ring) * records_per_step_ + c.rec;
+            } else if (conserved_by(index, f)) {
+                if (!cuda_ok(launch_totals(now_[static_cast<std::size_t>(f)], cells_, recs[j], partials_, counts_ + FE_MAX_OUT + 1, stream_), "totals",
+                        why)) {
+                    return false;
+                }
+            }
         }
     }
     for (int s = 0; s < count; ++s) {
         for (const gen::Launch& L : pp.stages) {
             if (!launch(L, sub_dt, 0, nullptr, why)) return false;
         }
-        int flags = 0;
-        if (s == 0) flags |= FE_PASS_BEFORE;
-        if (s == count - 1) flags |= FE_PASS_AFTER | FE_PASS_RANGE;
-        if (!launch(pp.gather, sub_dt, flags, check ? recs : nullptr, why)) return false;
+        const int flags = s == count - 1 ? FE_PASS_AFTER | FE_PASS_RANGE : 0;
+        if (!launch(pp.gather, sub_dt, flags, check ? recs : nullptr, why, s == 0 ? carried : nullptr)) return false;
         for (const int f : pp.swaps) std::swap(now_[static_cast<std::size_t>(f)], next_[static_cast<std::size_t>(f)]);
+    }
+    if (check) {
+        for (std::size_t j = 0; j < pp.gather.outs.size(); ++j) {
+            const int f = pp.gather.checked_fields[j];
+            if (f >= 0) carry_[static_cast<std::size_t>(f)] = Carry{pending.ring, rec_index[j], steps_};
+        }
     }
     flow_bounds(p, dt, count);
     tp.launches = launches_ - launches_before;
@@ -790,9 +826,11 @@ bool Engine::time_gather(int term, int launches, float& ms, std::string& why)
     const gen::ProgramPlan& pp = plan_.terms[static_cast<std::size_t>(term)];
     FeCheck* recs[FE_MAX_OUT] = {};
     for (std::size_t j = 0; j < pp.gather.outs.size(); ++j) recs[j] = records_ + j; // scratch records (ring slot 0)
+    // Ring slot 0 no longer holds what a carried total points at.
+    carry_.assign(carry_.size(), Carry{});
     cudaEventRecord(ev0_, stream_);
     for (int i = 0; i < launches; ++i) {
-        if (!launch(pp.gather, static_cast<float>(0.0), FE_PASS_BEFORE | FE_PASS_AFTER | FE_PASS_RANGE, recs, why)) return false;
+        if (!launch(pp.gather, static_cast<float>(0.0), FE_PASS_AFTER | FE_PASS_RANGE, recs, why)) return false;
     }
     cudaEventRecord(ev1_, stream_);
     if (!cuda_ok(cudaEventSynchronize(ev1_), "time", why)) return false;

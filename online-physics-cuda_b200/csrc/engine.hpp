@@ -100,7 +100,8 @@ private:
         std::vector<std::vector<std::vector<int>>> conserves; // per term: groups of fields
     };
 
-    bool launch(const gen::Launch& L, float dt, int flags, FeCheck* const* recs, std::string& why);
+    bool launch(const gen::Launch& L, float dt, int flags, FeCheck* const* recs, std::string& why, const FeCheck* const* carry = nullptr);
+    bool conserved_by(int term, int field) const;
     bool buffer(const gen::Buf& b, float*& out) const;
     bool map_for(const float* base, int bx, int by, FeTensorMap& out, std::string& why);
     CUfunction function(const std::string& name, unsigned smem, std::string& why);
@@ -149,6 +150,14 @@ private:
     std::vector<TermProfile> term_profile_;
     std::vector<Bounds> bounds_;
     std::vector<char> zero_;
+    // Per field: the record holding the totals of its current contents (ring slot, index, step), written by the checked
+    // gather that last wrote it; step -1 when none does (never checked, edited since, or written unchecked).
+    struct Carry {
+        int ring = -1;
+        int rec = -1;
+        long long step = -1;
+    };
+    std::vector<Carry> carry_;
     int launches_ = 0;
     double gpu_ms_ = 0.0;
     double compile_ms_ = 0.0;

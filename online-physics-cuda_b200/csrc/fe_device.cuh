@@ -46,17 +46,19 @@ struct FePassArgs {
     const float* src[FE_MAX_SRC];
     float* out[FE_MAX_OUT];
     FeCheck* rec[FE_MAX_OUT];  // null: this output is not checked in this pass
+    // The record of the pass that last wrote this output's field, whose totals after it are the totals before this
+    // pass: copied into rec's before/before_abs when the pass ends (null: they are already there, or not needed).
+    const FeCheck* carry[FE_MAX_OUT];
     float lo[FE_MAX_OUT];      // declared range of a checked output's field
     float hi[FE_MAX_OUT];
     double* partials;          // [FE_MAX_OUT][blocks][4]
     unsigned* count;           // [FE_MAX_OUT] blocks finished
     unsigned* err;
     float dt;
-    int flags;                 // FE_PASS_BEFORE | FE_PASS_AFTER
+    int flags;                 // FE_PASS_AFTER | FE_PASS_RANGE
     int zchunk;
     int blocks;
 };
-#define FE_PASS_BEFORE 1  // record the totals before the pass (the term's first substep)
 #define FE_PASS_AFTER 2   // record the totals after the pass (the term's last substep)
 #define FE_PASS_RANGE 4   // record range/NaN counts and bounds of what the pass writes (the term's last substep)
 
@@ -259,6 +261,110 @@ __device__ __forceinline__ void fe_acc_cell(FeAcc& a, float before, float after,
     a.changed |= (__float_as_uint(before) != __float_as_uint(after)) ? 1u : 0u;
 }
 
+// Per-thread contract accumulators of one checked output of a generated pass. The pass keeps the totals of what it
+// writes (sum and sum of |v|: FP64, from fp32 partials of the lane's cells of one plane), the bounds and the change
+// flag. The totals before the term are not summed here: they are the totals after the pass that last wrote the field
+// (FePassArgs::carry), or fe::launch_totals sums them first. The range/NaN test runs once a plane, on the bounds so far
+// and the plane's sum (a NaN or an infinity makes it non-finite); a plane that fails it is read back cell by cell, and
+// its bad cells are counted in the block's shared `fails` (out of range, not finite, ~index of the first).
+struct FeOutAcc {
+    double after, after_abs;
+    float pa, paa;  // this plane's fp32 partials of after and |after|
+    float lo, hi;   // least and most value so far (NaN ignored)
+    unsigned changed;
+};
+
+__device__ __forceinline__ void fe_out_init(FeOutAcc& a)
+{
+    a.after = 0.0; a.after_abs = 0.0;
+    a.pa = 0.f; a.paa = 0.f;
+    a.lo = __int_as_float(0x7f800000); a.hi = __int_as_float(0xff800000);
+    a.changed = 0u;
+}
+
+// Four consecutive cells: their values before the pass (for the change flag) and after it.
+__device__ __forceinline__ void fe_out_row4(FeOutAcc& a, const float* before, const float* after, bool range)
+{
+    a.pa += (after[0] + after[1]) + (after[2] + after[3]);
+    a.paa += (fabsf(after[0]) + fabsf(after[1])) + (fabsf(after[2]) + fabsf(after[3]));
+    if (range) {
+        a.lo = fminf(a.lo, fminf(fminf(after[0], after[1]), fminf(after[2], after[3])));
+        a.hi = fmaxf(a.hi, fmaxf(fmaxf(after[0], after[1]), fmaxf(after[2], after[3])));
+    }
+    a.changed |= ((__float_as_uint(before[0]) ^ __float_as_uint(after[0])) | (__float_as_uint(before[1]) ^ __float_as_uint(after[1])) |
+                     (__float_as_uint(before[2]) ^ __float_as_uint(after[2])) | (__float_as_uint(before[3]) ^ __float_as_uint(after[3]))) != 0u
+        ? 1u : 0u;
+}
+
+// Ends a plane: its partials into the FP64 totals. True when the plane may hold a bad cell (a bound past the declared
+// range, or a non-finite sum): the caller reads the plane's cells back. Once a cell is bad the bounds stay past the
+// range, so every later plane of the pass is read back too, and each bad cell is counted once, in its own plane.
+__device__ __forceinline__ bool fe_out_plane(FeOutAcc& a, float lo, float hi, bool range)
+{
+    const bool suspect = range && !(a.lo >= lo && a.hi <= hi && fabsf(a.pa) <= 3.0e38f);
+    a.after += static_cast<double>(a.pa);
+    a.after_abs += static_cast<double>(a.paa);
+    a.pa = 0.f;
+    a.paa = 0.f;
+    return suspect;
+}
+
+__device__ __forceinline__ void fe_out_bad(unsigned* fails, float v, unsigned index)
+{
+    atomicAdd(&fails[fe_not_finite(v) ? 1 : 0], 1u);
+    atomicMax(&fails[2], ~index);
+}
+
+// One cell (the plain passes): FP64 totals straight away, the range test per cell.
+__device__ __forceinline__ void fe_out_cell(FeOutAcc& a, float before, float after, float lo, float hi, unsigned index, bool range,
+    unsigned* fails)
+{
+    a.after += static_cast<double>(after);
+    a.after_abs += static_cast<double>(fabsf(after));
+    if (range) {
+        a.lo = fminf(a.lo, after);
+        a.hi = fmaxf(a.hi, after);
+        if (!(after >= lo && after <= hi)) fe_out_bad(fails, after, index);
+    }
+    a.changed |= (__float_as_uint(before) != __float_as_uint(after)) ? 1u : 0u;
+}
+
+// The block's output accumulators into its partial slot (fixed-order sums; the before slots stay zero), the order-free
+// parts into the record. Every thread of the block calls it; `fails` is the block's shared tally.
+__device__ __forceinline__ void fe_out_block(FeOutAcc& a, double* scratch, double* partial, FeCheck* rec, const unsigned* fails)
+{
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int warps = (blockDim.x + 31) >> 5;
+    const double s2 = fe_warp_sum(a.after);
+    const double s3 = fe_warp_sum(a.after_abs);
+    const unsigned lo = fe_warp_min(a.lo <= a.hi ? fe_order_key(a.lo) : 0xffffffffu);
+    const unsigned hi = fe_warp_max(a.lo <= a.hi ? fe_order_key(a.hi) : 0u);
+    const unsigned changed = __any_sync(0xffffffffu, a.changed != 0u) ? 1u : 0u;
+    if (lane == 0) {
+        scratch[4 * warp + 2] = s2;
+        scratch[4 * warp + 3] = s3;
+        if (lo != 0xffffffffu) atomicMax(&rec->lo_inv, ~lo);
+        if (hi != 0u) atomicMax(&rec->hi_key, hi);
+        if (changed && rec->changed == 0u) rec->changed = 1u;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t2 = 0.0, t3 = 0.0;
+        for (int w = 0; w < warps; ++w) {
+            t2 += scratch[4 * w + 2];
+            t3 += scratch[4 * w + 3];
+        }
+        partial[0] = 0.0;
+        partial[1] = 0.0;
+        partial[2] = t2;
+        partial[3] = t3;
+        if (fails[0]) atomicAdd(&rec->out_of_range, fails[0]);
+        if (fails[1]) atomicAdd(&rec->not_finite, fails[1]);
+        if (fails[2]) atomicMax(&rec->first_bad, fails[2]);
+    }
+}
+
 // The block's contract accumulators into its partial slot (fixed-order sums), plus the order-free integer parts
 // straight into the record. `scratch` holds 4 doubles per warp. Every thread of the block calls it.
 __device__ __forceinline__ void fe_acc_block(FeAcc& a, double* scratch, double* partial, FeCheck* rec)
@@ -310,7 +416,7 @@ __device__ __forceinline__ void fe_acc_block(FeAcc& a, double* scratch, double* 
 // changes, the order of the sum does not. `count` is reset for the next pass. Every thread of the block calls it;
 // `scratch` holds 4 doubles per warp.
 __device__ __forceinline__ void fe_acc_finish(const double* partials, int blocks, unsigned* count, double* scratch,
-    FeCheck* rec, bool totals_before, bool totals_after)
+    FeCheck* rec, bool totals_before, bool totals_after, const FeCheck* carry = nullptr)
 {
     __shared__ unsigned last;
     __threadfence();
@@ -356,7 +462,11 @@ __device__ __forceinline__ void fe_acc_finish(const double* partials, int blocks
             s2 += scratch[4 * w + 2];
             s3 += scratch[4 * w + 3];
         }
-        if (totals_before) {
+        if (carry != nullptr) {
+            // The totals after the pass that last wrote the field are the totals before this one.
+            rec->before = carry->after;
+            rec->before_abs = carry->after_abs;
+        } else if (totals_before) {
             rec->before = s0;
             rec->before_abs = s1;
         }
@@ -445,16 +555,16 @@ struct FePlainCtx {
 };
 
 template <class P>
-__device__ __forceinline__ void fe_pass_contracts(FeAcc* acc, double* scratch, const FePassArgs& a)
+__device__ __forceinline__ void fe_pass_contracts(FeOutAcc* acc, double* scratch, unsigned (*fails)[3], const FePassArgs& a)
 {
     const int block = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     const int blocks = gridDim.x * gridDim.y * gridDim.z;
 #pragma unroll
     for (int j = 0; j < P::NOUT; ++j) {
         if (P::checked(j) && a.rec[j] != nullptr) {
-            fe_acc_block(acc[j], scratch, a.partials + 4 * (static_cast<fe_u64>(j) * blocks + block), a.rec[j]);
-            fe_acc_finish(a.partials + 4 * static_cast<fe_u64>(j) * blocks, blocks, a.count + j, scratch, a.rec[j],
-                (a.flags & FE_PASS_BEFORE) != 0, (a.flags & FE_PASS_AFTER) != 0);
+            fe_out_block(acc[j], scratch, a.partials + 4 * (static_cast<fe_u64>(j) * blocks + block), a.rec[j], fails[j]);
+            fe_acc_finish(a.partials + 4 * static_cast<fe_u64>(j) * blocks, blocks, a.count + j, scratch, a.rec[j], false,
+                (a.flags & FE_PASS_AFTER) != 0, a.carry[j]);
         }
     }
 }
@@ -468,6 +578,7 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
     extern __shared__ __align__(128) float fe_sm[];
     __shared__ __align__(8) fe_u64 bar[P::NST];
     __shared__ double scratch[4 * P::W];
+    __shared__ unsigned fails[P::NOUT][3];
     static_assert(P::NST >= 2 * P::RZ + 2, "the ring holds 2 RZ + 1 planes and the one being fetched");
     const int x0 = blockIdx.x * 128;
     const int y0 = blockIdx.y * (P::W * P::R);
@@ -489,15 +600,16 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
     };
     int issued = 0;
     if (threadIdx.x == 0) {
+        for (int j = 0; j < P::NOUT; ++j) fails[j][0] = fails[j][1] = fails[j][2] = 0u;
         for (int s = 0; s < P::NST; ++s) fe_mbar_init(&bar[s], 1);
         fe_fence_mbar_init();
         issued = min(P::NST, nplanes);
         for (int j = 0; j < issued; ++j) issue(j);
     }
     __syncthreads();
-    FeAcc acc[P::NOUT];
+    FeOutAcc acc[P::NOUT];
 #pragma unroll
-    for (int j = 0; j < P::NOUT; ++j) fe_acc_init(acc[j]);
+    for (int j = 0; j < P::NOUT; ++j) fe_out_init(acc[j]);
     // Every thread waits (bounded) for the planes a z needs, and evens the x edge of each plane that landed (XFILL);
     // the barrier that follows makes both visible and, OR-ing the outcomes, the decision to go on uniform. The next
     // plane to wait for is tracked by its stage and phase, stepped rather than divided.
@@ -533,8 +645,6 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         if (y < P::NY && x < P::NX) live |= 1u << r;
         if (y - P::RYT >= 0 && y + P::RYT < P::NY) yin |= 1u << r;
     }
-    const bool totals_before = (a.flags & FE_PASS_BEFORE) != 0;
-    const bool totals_after = (a.flags & FE_PASS_AFTER) != 0;
     const bool range = (a.flags & FE_PASS_RANGE) != 0;
     const fe_u64 row0 = static_cast<fe_u64>(P::NX) * static_cast<fe_u64>(y0 + warp * P::R) + static_cast<fe_u64>(x);
     // The ring stage of plane z, stepped with z; planes whose z reach stays in the lattice take their neighbours'
@@ -582,12 +692,27 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
                 if (P::checked(j) && a.rec[j] != nullptr) {
                     const float bb[4] = {b[0][j], b[1][j], b[2][j], b[3][j]};
                     const float oo[4] = {o[0][j], o[1][j], o[2][j], o[3][j]};
-                    fe_acc_row4(acc[j], bb, oo, a.lo[j], a.hi[j], static_cast<unsigned>(at), totals_before, totals_after, range);
+                    fe_out_row4(acc[j], bb, oo, range);
                 }
             }
         }
 #pragma unroll
-        for (int j = 0; j < P::NOUT; ++j) fe_acc_flush(acc[j]);
+        for (int j = 0; j < P::NOUT; ++j) {
+            if (P::checked(j) && a.rec[j] != nullptr && fe_out_plane(acc[j], a.lo[j], a.hi[j], range)) {
+                // Read this lane's cells of the plane back (its own stores, through L2) and tally the bad ones.
+#pragma unroll
+                for (int r = 0; r < P::R; ++r) {
+                    if (ragged && !((live >> r) & 1u)) continue;
+                    const fe_u64 at = plane0 + static_cast<fe_u64>(r) * P::NX;
+                    const float4 v4 = __ldcg(reinterpret_cast<const float4*>(a.out[j] + at));
+                    const float v[4] = {v4.x, v4.y, v4.z, v4.w};
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (!(v[q] >= a.lo[j] && v[q] <= a.hi[j])) fe_out_bad(fails[j], v[q], static_cast<unsigned>(at) + q);
+                    }
+                }
+            }
+        }
         if (z + 1 < ze) wait_upto(min(z + 1 + P::RZ, P::NZ - 1) - zlo);
         failed = __syncthreads_or(ok ? 0 : 1) != 0;
         const int release = z - P::RZ - zlo;
@@ -605,7 +730,7 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         }
         return;
     }
-    fe_pass_contracts<P>(acc, scratch, a);
+    fe_pass_contracts<P>(acc, scratch, fails, a);
 }
 
 // The plain pass: a thread a (x, y) column marching a chunk of z-planes, reads through the read-only path.
@@ -613,14 +738,18 @@ template <class P>
 __device__ __forceinline__ void fe_plain_pass(const FePassArgs& a)
 {
     __shared__ double scratch[4 * 8];
+    __shared__ unsigned fails[P::NOUT][3];
     const int x = blockIdx.x * 32 + (threadIdx.x & 31);
     const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
     const bool live = x < P::NX && y < P::NY;
     const int zb = blockIdx.z * a.zchunk;
     const int ze = min(P::NZ, zb + a.zchunk);
-    FeAcc acc[P::NOUT];
+    if (threadIdx.x < 3 * P::NOUT) fails[threadIdx.x / 3][threadIdx.x % 3] = 0u;
+    __syncthreads();
+    const bool range = (a.flags & FE_PASS_RANGE) != 0;
+    FeOutAcc acc[P::NOUT];
 #pragma unroll
-    for (int j = 0; j < P::NOUT; ++j) fe_acc_init(acc[j]);
+    for (int j = 0; j < P::NOUT; ++j) fe_out_init(acc[j]);
     FePlainCtx<P> c;
     c.src = a.src;
     c.dt = a.dt;
@@ -633,12 +762,11 @@ __device__ __forceinline__ void fe_plain_pass(const FePassArgs& a)
         for (int j = 0; j < P::NOUT; ++j) {
             a.out[j][at] = o[j];
             if (P::checked(j) && a.rec[j] != nullptr) {
-                fe_acc_cell(acc[j], b[j], o[j], a.lo[j], a.hi[j], static_cast<unsigned>(at), (a.flags & FE_PASS_BEFORE) != 0,
-                    (a.flags & FE_PASS_AFTER) != 0, (a.flags & FE_PASS_RANGE) != 0);
+                fe_out_cell(acc[j], b[j], o[j], a.lo[j], a.hi[j], static_cast<unsigned>(at), range, fails[j]);
             }
         }
     }
-    fe_pass_contracts<P>(acc, scratch, a);
+    fe_pass_contracts<P>(acc, scratch, fails, a);
 }
 
 // A deterministic reduction of one expression over the lattice (maxof / minof / sumof): a fixed assignment of cells to

@@ -119,6 +119,78 @@ def test_range_and_nan_violations_are_reported(cuda):
     s.close()
 
 
+@pytest.mark.parametrize("nx", [16, 128])
+def test_conserved_totals_carry_from_step_to_step(cuda, nx):
+    """The totals before a term are those after the checked pass that last wrote the field (carried, exactly), or
+    summed afresh on the first step and after an edit; either way they are the field's FP64 sums (plain pass at 16 wide,
+    TMA slab pass with ragged rows at 128)."""
+    from fieldcuda.solver import Solver
+    law = ("field T init 1 range -1e6 1e6\nparam leak = 0.5\nterm leaky\n  d T = diffuse(1, T) - leak * T\n  conserves T\n")
+    s = Solver(law, nx, 12, 8, 0.1)
+    T0 = np.random.default_rng(0).uniform(1, 2, (8, 12, nx)).astype(np.float32)
+    s.set_field("T", T0)
+
+    def leak_record():
+        v = [x for x in s.violations() if x.kind == "conservation"]
+        assert len(v) == 1, s.violations()
+        return v[0]
+
+    s.step(0.001)
+    first = leak_record()
+    assert abs(first.before - T0.astype(np.float64).sum()) <= 1e-7 * abs(first.before)
+    T1 = s.values("T")
+    assert abs(first.after - T1.astype(np.float64).sum()) <= 1e-7 * abs(first.after)
+    s.step(0.001)
+    second = leak_record()
+    assert second.before == first.after
+    s.set_param("leak", 0.0)
+    s.step(0.001)
+    assert not s.violations()
+    s.set_param("leak", 0.5)
+    s.set_field("T", T0)  # an edit: the totals are summed again
+    s.step(0.001)
+    again = leak_record()
+    assert abs(again.before - T0.astype(np.float64).sum()) <= 1e-7 * abs(again.before)
+    s.check_contracts_every(2)  # steps 4 and 6 checked, 5 not: step 6 sums its totals again
+    s.step(0.001)
+    s.step(0.001)
+    T5 = s.values("T")
+    s.step(0.001)
+    late = leak_record()
+    assert abs(late.before - T5.astype(np.float64).sum()) <= 1e-7 * abs(late.before)
+    s.close()
+
+
+@pytest.mark.parametrize("nx", [16, 128])
+def test_range_cells_are_counted_once_across_planes(cuda, nx):
+    """Out-of-range and NaN cells scattered over several planes: each counted once, the first one named (on the slab
+    pass the test runs per plane, and a plane that fails it is read back)."""
+    from fieldcuda.solver import Solver
+    law = "field a init 0 range -1 1\nfield b init 0 range -1e30 1e30 static\nterm t\n  d a = b\n"
+    shape = (6, 20, nx)
+    s = Solver(law, nx, 20, 6, 1.0)
+    b = np.zeros(shape, np.float32)
+    bad = [(1, 3, 5), (1, 19, nx - 1), (4, 0, 7), (5, 11, nx - 2)]
+    for z, y, x in bad:
+        b[z, y, x] = 5.0
+    b[3, 7, 2] = np.nan
+    s.set_field("b", b)
+    s.step(1.0)
+    v = sorted(s.violations(), key=lambda x: x.kind)
+    kinds = {x.kind: x for x in v}
+    assert set(kinds) == {"not-finite"}, v
+    nan = kinds["not-finite"]
+    assert nan.count == len(bad) + 1
+    assert nan.first_cell == 5 + nx * (3 + 20 * 1)
+    b[3, 7, 2] = 0.0
+    s.set_field("b", b)
+    s.set_field("a", np.zeros(shape, np.float32))
+    s.step(1.0)
+    v = s.violations()
+    assert len(v) == 1 and v[0].kind == "range" and v[0].count == len(bad) and v[0].first_cell == 5 + nx * (3 + 20 * 1), v
+    s.close()
+
+
 def test_substep_cap_and_ignoring_max_dt(cuda):
     from fieldcuda.solver import Solver
     law = "field T init 0 range -1e9 1e9\nterm c\n  d T = diffuse(1, T)\n  max_dt = 0.1 * h * h\n"
