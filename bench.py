@@ -659,7 +659,7 @@ def run_ours(args, world, rank, local):
 
 def profile_case(name):
     """Small cases of the kernels the profiles under profiles/ summarise, for ncu (one GPU; a few launches):
-    heat        the heat law on 384^3 (inputs larger than L2), 3 steps: the generated gather;
+    heat        the heat law on 512^3 (the bench's lattice; inputs larger than L2), 3 steps: the generated gather;
     heston      36 options on 512 x 256, 16 Douglas steps, split (16, 4, 512): the cluster kernel;
     corrector   3 training steps, one gradient and one guarded apply on 256 x 32 x 32 cells: the tcgen05 kernels;
     multifield  the 43-term law on 128^3, 3 steps: its generated passes."""
@@ -687,7 +687,7 @@ def profile_case(name):
     elif name == "heat":
         from fieldcuda.solver import Solver
         from oracle import heat as oh
-        n = 384
+        n = 512
         h = 1.0 / n
         s = Solver(HEAT_LAW, n, n, n, h, "heat.law")
         s.set_field("T", oh.gaussian_blobs(n, h, seed=0))
@@ -726,7 +726,7 @@ def main():
     ap.add_argument("--no-multifield", action="store_true", help="skip the 43-term multi-field law section")
     ap.add_argument("--no-calibration", action="store_true", help="skip the adjoint calibration section")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-correction section")
-    ap.add_argument("--profile-case", default="", help="run one small case for ncu (heston, corrector, multifield) and exit")
+    ap.add_argument("--profile-case", default="", help="run one small case for ncu (heat, heston, corrector, multifield) and exit")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)

@@ -128,7 +128,7 @@ bool Engine::create(const std::vector<law::Source>& sources, int nx, int ny, int
 
     // Contract records: one per checked output of every program, per step, in a ring.
     records_per_step_ = 0;
-    std::size_t partial_doubles = 4 * 1024;
+    std::size_t partial_doubles = std::max<std::size_t>(4 * 1024, 4 * static_cast<std::size_t>(kTotalsBlocks));
     auto consider = [&](const gen::Launch& L) {
         const bool slab = L.slab;
         const int zchunk = zchunk_for(L, slab);

@@ -38,8 +38,9 @@ inline float exact_reciprocal(float v)
 cudaError_t launch_heat7_tma(int variant, const FeTensorMap& map, const HeatArgs& a, cudaStream_t stream);
 cudaError_t launch_heat7_plain(const float* T, const HeatArgs& a, cudaStream_t stream);
 cudaError_t launch_fill(float* p, size_t n, float v, int sms, cudaStream_t stream);
-// Sum and sum of |v| of n cells into rec->before / before_abs (totals.cu): kTotalsBlocks blocks, 4 partial doubles each.
-constexpr int kTotalsBlocks = 296;
+// Sum and sum of |v| of n cells (a 16-byte aligned buffer) into rec->before / before_abs (totals.cu): kTotalsBlocks blocks,
+// 4 partial doubles each.
+constexpr int kTotalsBlocks = 1184;
 cudaError_t launch_totals(const float* v, size_t n, FeCheck* rec, double* partials, unsigned* count, cudaStream_t stream);
 cudaError_t launch_copy(const float* a, float* b, size_t n, int sms, cudaStream_t stream);
 int heat7_tma_rows(int variant);

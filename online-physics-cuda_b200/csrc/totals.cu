@@ -13,12 +13,26 @@ namespace fe {
 __global__ void __launch_bounds__(256) totals_f32(const float* __restrict__ v, size_t n, FeCheck* rec, double* partials, unsigned* count)
 {
     __shared__ double scratch[4 * 8];
-    const size_t per = (n + gridDim.x - 1) / gridDim.x;
+    // Block b sums cells [b0, b1): a whole number of float4s (the buffer is 256-byte aligned), the last block the tail.
+    const size_t per = ((n + gridDim.x - 1) / gridDim.x + 3) / 4 * 4;
     const size_t b0 = min(n, per * blockIdx.x);
     const size_t b1 = min(n, b0 + per);
+    const float4* v4 = reinterpret_cast<const float4*>(v);
     FeAcc acc;
     fe_acc_init(acc);
-    for (size_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+#pragma unroll 4
+    for (size_t i = b0 / 4 + threadIdx.x; i < b1 / 4; i += blockDim.x) {
+        const float4 x = __ldg(v4 + i);
+        acc.before += static_cast<double>(x.x);
+        acc.before += static_cast<double>(x.y);
+        acc.before += static_cast<double>(x.z);
+        acc.before += static_cast<double>(x.w);
+        acc.before_abs += fabs(static_cast<double>(x.x));
+        acc.before_abs += fabs(static_cast<double>(x.y));
+        acc.before_abs += fabs(static_cast<double>(x.z));
+        acc.before_abs += fabs(static_cast<double>(x.w));
+    }
+    for (size_t i = b1 / 4 * 4 + threadIdx.x; i < b1; i += blockDim.x) {
         const double x = static_cast<double>(v[i]);
         acc.before += x;
         acc.before_abs += fabs(x);
