@@ -8,8 +8,9 @@ copy roof.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--size 512]
 
-Prints ONE JSON line (rank 0). With --gpus N > 1 (torchrun), every rank steps its own 512^3 lattice (independent
-instances, no data-path collective: weak scaling), timed with CUDA events, max over ranks.
+Prints ONE JSON line (rank 0). With --gpus N > 1 (torchrun), the lattice is 512 x 512 x 512N, one 512-plane z-slab a
+rank (weak scaling): each rank steps its slab plus one halo plane a side, the halo planes are exchanged over NCCL after
+every step and conservation is judged over the ranks (fieldcuda/slabs.py); timed with CUDA events, max over ranks.
 """
 import argparse
 import ctypes
@@ -541,15 +542,39 @@ def run_ours(args, world, rank, local):
     pinned_in = torch.from_numpy(T0).pin_memory()
     pinned_out = torch.empty((n, n, n), dtype=torch.float32).pin_memory()
 
-    # The product path: the law compiled by the backend (IR -> sm_100a kernels), stepped through the C ABI.
-    s = Solver(HEAT_LAW, n, n, n, h, "heat.law")
-    s.set_field("T", pinned_in.numpy())
+    # The product path: the law compiled by the backend (IR -> sm_100a kernels), stepped through the C ABI. On N GPUs
+    # the lattice is n x n x (N n), one z-slab of n planes a rank, halo planes exchanged over NCCL after every step
+    # and conservation judged over the ranks (fieldcuda/slabs.py).
+    if world > 1:
+        from fieldcuda.slabs import DistComm, SlabLaw
+        slab = SlabLaw(HEAT_LAW, n, n, n * world, h, rank, world, DistComm(), source_name="heat.law")
+        s = slab.solver
+        stepper = slab
+    else:
+        slab = None
+        s = Solver(HEAT_LAW, n, n, n, h, "heat.law")
+        stepper = s
+    local_cells = n * n * s.shape[0]
+
+    def judge():
+        if slab is not None:
+            return slab.sync()
+        s.sync()
+        return s.violations()
+
+    def upload():
+        if slab is not None:
+            slab.set_field("T", pinned_in.numpy())
+        else:
+            s.set_field("T", pinned_in.numpy())
+
+    upload()
     stream = torch.cuda.ExternalStream(s.stream)
     s.set_deferred(True)  # contracts checked every step, judged after the run: no step waits for the host
     for _ in range(W):
-        s.step(dt)
-    s.sync()
-    assert not s.violations(), s.violations()
+        stepper.step(dt)
+    broken = judge()
+    assert not broken, broken
 
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
@@ -559,15 +584,14 @@ def run_ours(args, world, rank, local):
     e0.record(stream)
     launches = 0
     for _ in range(K):
-        s.step(dt)
+        stepper.step(dt)
         launches += s.profile()["launches"]
     e1.record(stream)
     stream.synchronize()
     barrier(world)
     clk = clocks.stop()
     ms_total = max_over_ranks(world, e0.elapsed_time(e1))
-    s.sync()  # judge every timed step's contracts (conserved total, range, NaN)
-    broken = s.violations()
+    broken = judge()  # judge every timed step's contracts (conserved total, range, NaN)
     assert not broken, broken
 
     # The dominant kernel alone: the generated gather pass (one launch a step), timed back to back.
@@ -575,16 +599,20 @@ def run_ours(args, world, rank, local):
 
     # End to end through the public API with host buffers: the state up from pinned host memory, K steps each judged
     # on the host (its contract records read back), the state back down to pinned host memory.
-    s.set_deferred(False)
+    s.set_deferred(slab is not None)  # one GPU: each step judged on the host; slabs: judged over the ranks at the end
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    s.set_field("T", pinned_in.numpy())
+    upload()
     for _ in range(K):
-        s.step(dt)
-    _lib.check(_lib.lib().fe_law_fetch(s._h, 0, ctypes.c_void_p(pinned_out.data_ptr())))
+        stepper.step(dt)
+    if slab is not None:
+        pinned_out.numpy()[:] = slab.values("T")
+    else:
+        _lib.check(_lib.lib().fe_law_fetch(s._h, 0, ctypes.c_void_p(pinned_out.data_ptr())))
+    broken = judge()
     e2e_ms = max_over_ranks(world, (time.perf_counter() - t0) * 1e3)
-    assert not s.violations(), s.violations()
+    assert not broken, broken
     s.close()
 
     side = torch.cuda.Stream()
@@ -596,7 +624,7 @@ def run_ours(args, world, rank, local):
     value = BYTES_PER_CELL * total_cells * K / (ms_total * 1e-3) / 1e9
     e2e_value = BYTES_PER_CELL * total_cells * K / (e2e_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peak()
-    achieved = BYTES_PER_CELL * cells / (gather_ms * 1e-3) / 1e9
+    achieved = BYTES_PER_CELL * local_cells / (gather_ms * 1e-3) / 1e9
     traffic = profile_traffic("heat_gather_512.md")
 
     cpu = None
@@ -634,8 +662,9 @@ def run_ours(args, world, rank, local):
         "value": value, "unit": "GB/s", "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: sum of 4 seeded Gaussian blobs (numpy default_rng(rank))",
-        "config": {"workload": f"heat law d T = diffuse(1, T), conserves T, {n}^3 fp32, h = 1/{n}, dt = 0.4 h^2/6 "
-                               f"(1 substep), contracts checked every step", "cells_per_gpu": cells,
+        "config": {"workload": f"heat law d T = diffuse(1, T), conserves T, {n}^3 fp32 a GPU (on N GPUs one {n} x {n} x {n}N "
+                               f"lattice in z-slabs, halo planes over NCCL), h = 1/{n}, dt = 0.4 h^2/6 (1 substep), "
+                               f"contracts checked every step", "cells_per_gpu": cells,
                    "path": "fe_law_step (law text -> IR -> generated sm_100a TMA pass)",
                    "l2": "inputs larger than L2 (512 MiB a buffer)",
                    "handwritten_kernel_gbs": BYTES_PER_CELL * cells / (hand_ms * 1e-3) / 1e9},

@@ -114,6 +114,17 @@ typedef struct fe_violation {
     char detail[160];
 } fe_violation;
 
+/* One conserves group's totals over one checked step, for a judge outside the handle (fe_law_take_totals). */
+typedef struct fe_group_totals {
+    long long step;      /* the step (0-based) */
+    int term;            /* the term's index */
+    int group;           /* the conserves group's index within the term */
+    int substeps;        /* substeps the term took */
+    int reserved;
+    double before, after; /* sum of the group's fields before the term and after it, over the owned planes */
+    double scale;        /* sum of |v| before the term (the tolerance scale, Solver.cpp:439-453) */
+} fe_group_totals;
+
 typedef struct fe_step_info {
     int violations;      /* violations now held (fe_law_violation) */
     int launches;        /* kernels the step launched */
@@ -171,6 +182,22 @@ int fe_law_fetch_device(fe_law* law, int field, float* dev);
  * its last step: the backend forgets what it knew of the field's bounds (no counterpart in the reference, whose host
  * FieldSet is written through FieldEdits instead). */
 int fe_law_mark_edited(fe_law* law, int field);
+
+/* A lattice split along z over ranks (no counterpart in the reference, whose CudaSolver runs one lattice on one GPU;
+ * SURVEY's multi-GPU form of CudaSolver::step). A rank's handle holds its slab plus halo planes copied from its
+ * neighbours after every step:
+ *   fe_law_set_owned_z: contracts (totals, bounds, range, change flag) cover planes [z0, z1) only;
+ *   fe_law_mark_halo: the field's halo planes were written by the caller (its bounds are forgotten, the owned totals kept);
+ *   fe_law_set_external_conservation: checked steps log each conserves group's totals (fe_law_take_totals, which hands
+ *     over and clears the log, at most `max`, *n the count) instead of judging them: the caller sums over ranks;
+ *   fe_law_plan_z_reach: for law text on a lattice (planned, not compiled): planes along z one step reads beyond a cell
+ *     (*reach, summed over the step's passes) and flags: 1 the law reduces over the lattice, 2 it solves along z
+ *     (neither splits into slabs). */
+int fe_law_set_owned_z(fe_law* law, int z0, int z1);
+int fe_law_mark_halo(fe_law* law, int field);
+int fe_law_set_external_conservation(fe_law* law, int on);
+int fe_law_take_totals(fe_law* law, fe_group_totals* out, int max, int* n);
+int fe_law_plan_z_reach(const char* law_text, int nx, int ny, int nz, double h, int* reach, int* flags);
 int fe_law_field_device_ptr(const fe_law* law, int field, const float** dev);
 
 /* One step of dt: every term in declaration order with its substeps, then the derives (Solver::step,

@@ -241,6 +241,62 @@ int fe_law_mark_edited(fe_law* law, int field)
     return fe::ok();
 }
 
+int fe_law_set_owned_z(fe_law* law, int z0, int z1)
+{
+    if (law == nullptr) return fe::fail(FE_EINVAL, "null handle");
+    if (!law->engine.set_owned_z(z0, z1)) return fe::fail(FE_EINVAL, "fe_law_set_owned_z: need 0 <= z0 < z1 <= nz");
+    return fe::ok();
+}
+
+int fe_law_mark_halo(fe_law* law, int field)
+{
+    if (!field_ok(law, field)) return fe::fail(FE_EINVAL, "bad field");
+    law->engine.mark_halo(field);
+    return fe::ok();
+}
+
+int fe_law_set_external_conservation(fe_law* law, int on)
+{
+    if (law == nullptr) return fe::fail(FE_EINVAL, "null handle");
+    law->engine.set_external_conservation(on != 0);
+    return fe::ok();
+}
+
+int fe_law_take_totals(fe_law* law, fe_group_totals* out, int max, int* n)
+{
+    if (law == nullptr || n == nullptr || max < 0 || (max > 0 && out == nullptr)) return fe::fail(FE_EINVAL, "fe_law_take_totals: bad arguments");
+    const std::vector<fe::GroupTotals> all = law->engine.take_totals();
+    if (static_cast<int>(all.size()) > max) return fe::fail(FE_EINVAL, "fe_law_take_totals: " + std::to_string(all.size()) + " entries, room for " + std::to_string(max));
+    for (std::size_t i = 0; i < all.size(); ++i) {
+        std::memset(&out[i], 0, sizeof(out[i]));
+        out[i].step = all[i].step;
+        out[i].term = all[i].term;
+        out[i].group = all[i].group;
+        out[i].substeps = all[i].substeps;
+        out[i].before = all[i].before;
+        out[i].after = all[i].after;
+        out[i].scale = all[i].scale;
+    }
+    *n = static_cast<int>(all.size());
+    return fe::ok();
+}
+
+int fe_law_plan_z_reach(const char* law_text, int nx, int ny, int nz, double h, int* reach, int* flags)
+{
+    if (reach == nullptr || flags == nullptr) return fe::fail(FE_EINVAL, "null argument");
+    fe::law::Law law;
+    std::string why;
+    if (!compile_law(law_text, law, why)) return fe::fail(FE_ELAW, why);
+    if (nx < 1 || ny < 1 || nz < 1 || !(h > 0.0)) return fe::fail(FE_EINVAL, "bad lattice");
+    const fe::ir::Module m = fe::ir::lower(law);
+    fe::gen::Plan plan;
+    if (!fe::gen::generate(m, law, nx, ny, nz, h, plan, why)) return fe::fail(FE_EUNSUP, why);
+    bool reductions = false, z_solves = false;
+    fe::plan_z_reach(plan, *reach, reductions, z_solves);
+    *flags = (reductions ? 1 : 0) | (z_solves ? 2 : 0);
+    return fe::ok();
+}
+
 int fe_law_field_device_ptr(const fe_law* law, int field, const float** dev)
 {
     if (!field_ok(law, field) || dev == nullptr) return fe::fail(FE_EINVAL, "bad field");

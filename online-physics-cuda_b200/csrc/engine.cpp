@@ -115,6 +115,8 @@ bool Engine::create(const std::vector<law::Source>& sources, int nx, int ny, int
     bounds_.assign(fields, Bounds{});
     zero_.assign(fields, 0);
     carry_.assign(fields, Carry{});
+    own_z0_ = 0;
+    own_z1_ = nz;
     for (std::size_t f = 0; f < fields; ++f) {
         const float init = static_cast<float>(law_.fields[f].init);
         if (!cuda_ok(launch_fill(now_[f], cells_, init, sms_, stream_), "fill", why)) return false;
@@ -243,6 +245,8 @@ bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* r
         a.lo[j] = f >= 0 ? static_cast<float>(law_.fields[static_cast<std::size_t>(f)].lo) : -3.0e38f;
         a.hi[j] = f >= 0 ? static_cast<float>(law_.fields[static_cast<std::size_t>(f)].hi) : 3.0e38f;
     }
+    a.own_z0 = own_z0_;
+    a.own_z1 = own_z1_;
     a.partials = partials_;
     a.count = counts_;
     a.err = counts_ + FE_MAX_OUT;
@@ -346,6 +350,50 @@ bool Engine::upload(int field, const void* src, bool device, std::string& why)
     zero_[static_cast<std::size_t>(field)] = (b.lo == 0.0 && b.hi == 0.0) ? 1 : 0;
     carry_[static_cast<std::size_t>(field)] = Carry{};
     return true;
+}
+
+void Engine::mark_halo(int field)
+{
+    if (field < 0 || static_cast<std::size_t>(field) >= now_.size()) return;
+    bounds_[static_cast<std::size_t>(field)] = Bounds{};
+    zero_[static_cast<std::size_t>(field)] = 0;
+}
+
+bool Engine::set_owned_z(int z0, int z1)
+{
+    if (z0 < 0 || z1 > nz_ || z0 >= z1) return false;
+    // The totals of a field's current contents were taken over the old range.
+    carry_.assign(carry_.size(), Carry{});
+    own_z0_ = z0;
+    own_z1_ = z1;
+    return true;
+}
+
+std::vector<GroupTotals> Engine::take_totals()
+{
+    std::vector<GroupTotals> out;
+    out.swap(totals_log_);
+    return out;
+}
+
+void plan_z_reach(const gen::Plan& plan, int& reach, bool& reductions, bool& z_solves)
+{
+    reach = 0;
+    reductions = false;
+    z_solves = false;
+    auto count = [&](const gen::Launch& L) {
+        if (L.kind == gen::Launch::Pass) reach += L.rz;
+        if (L.kind == gen::Launch::Reduce) reductions = true;
+        if (L.kind == gen::Launch::TridiagYZ && L.axis == 2) z_solves = true;
+    };
+    for (const auto* progs : {&plan.terms, &plan.derives}) {
+        for (const gen::ProgramPlan& pp : *progs) {
+            if (pp.empty) continue;
+            for (const gen::Launch& L : pp.stages) count(L);
+            for (const gen::Launch& L : pp.limit) count(L);
+            count(pp.gather);
+        }
+    }
 }
 
 void Engine::mark_edited(int field)
@@ -619,8 +667,10 @@ bool Engine::run_program(int index, const ir::Program& p, const gen::ProgramPlan
             if (c.step >= 0 && steps_ - c.step < ring_ - 2) {
                 carried[j] = records_ + static_cast<std::size_t>(c.ring) * records_per_step_ + c.rec;
             } else if (conserved_by(index, f)) {
-                if (!cuda_ok(launch_totals(now_[static_cast<std::size_t>(f)], cells_, recs[j], partials_, counts_ + FE_MAX_OUT + 1, stream_), "totals",
-                        why)) {
+                const std::size_t plane = static_cast<std::size_t>(nx_) * ny_;
+                if (!cuda_ok(launch_totals(now_[static_cast<std::size_t>(f)] + plane * own_z0_, plane * (own_z1_ - own_z0_), recs[j], partials_,
+                                 counts_ + FE_MAX_OUT + 1, stream_),
+                        "totals", why)) {
                     return false;
                 }
             }
@@ -778,6 +828,11 @@ bool Engine::judge(PendingStep& pending, std::string& why)
                 }
             }
             if (!any) continue; // the term was idle: nothing moved
+            if (external_conservation_) {
+                totals_log_.push_back(GroupTotals{pending.step, static_cast<int>(t), static_cast<int>(&group - term.conserves.data()), substeps, before,
+                    after, scale});
+                continue;
+            }
             const double tolerance = 1e-5 * (scale + 1.0) * std::sqrt(static_cast<double>(substeps));
             if (std::abs(after - before) > tolerance) {
                 Violation v;

@@ -37,6 +37,20 @@ struct Bounds {
     [[nodiscard]] bool none() const { return lo == 0.0 && hi == 0.0; }
 };
 
+// The totals of one conserves group over one checked step, kept for a judge outside the engine (a lattice split in
+// z-slabs over ranks is conserved as a whole, not slab by slab).
+struct GroupTotals {
+    long long step = 0;
+    int term = 0;
+    int group = 0;
+    int substeps = 1;
+    double before = 0.0, after = 0.0, scale = 0.0;
+};
+
+// How many planes along z one step of a planned law reads beyond a cell (the sum over its passes, in order), and whether
+// it reduces over the lattice or solves along z (neither splits into z-slabs).
+void plan_z_reach(const gen::Plan& plan, int& reach, bool& reductions, bool& z_solves);
+
 struct TermProfile {
     int launches = 0;
     int substeps = 0;
@@ -53,6 +67,14 @@ public:
     // A field's cells were changed in place on the device by someone else (ordered on the engine's stream): what the
     // engine knew of its bounds no longer holds.
     void mark_edited(int field);
+    // Halo planes of a field (outside the owned z-range) were written by someone else: its bounds are unknown, while
+    // the totals of the owned planes still hold.
+    void mark_halo(int field);
+    // Contracts (totals, bounds, range, change) cover planes [z0, z1) only: the rest are halo planes another rank owns.
+    bool set_owned_z(int z0, int z1);
+    // Conservation is judged outside: each checked step's group totals go to a log instead (take_totals).
+    void set_external_conservation(bool on) { external_conservation_ = on; }
+    std::vector<GroupTotals> take_totals();
     bool fetch(int field, void* dst, bool device, std::string& why);
     const float* device_field(int field) const { return now_[static_cast<std::size_t>(field)]; }
 
@@ -158,6 +180,9 @@ private:
         long long step = -1;
     };
     std::vector<Carry> carry_;
+    int own_z0_ = 0, own_z1_ = 0;
+    bool external_conservation_ = false;
+    std::vector<GroupTotals> totals_log_;
     int launches_ = 0;
     double gpu_ms_ = 0.0;
     double compile_ms_ = 0.0;

@@ -58,6 +58,7 @@ struct FePassArgs {
     int flags;                 // FE_PASS_AFTER | FE_PASS_RANGE
     int zchunk;
     int blocks;
+    int own_z0, own_z1;        // contracts cover planes [own_z0, own_z1) (the rest: halo planes another rank owns)
 };
 #define FE_PASS_AFTER 2   // record the totals after the pass (the term's last substep)
 #define FE_PASS_RANGE 4   // record range/NaN counts and bounds of what the pass writes (the term's last substep)
@@ -651,6 +652,7 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
     // stages from it, the clamped ones at the lattice's z ends recompute them.
     int sz = zb - zlo;
     for (int z = zb; z < ze && !failed; ++z) {
+        const bool own = z >= a.own_z0 && z < a.own_z1;
         FeSlabCtx<P> c;
         c.sm = fe_sm;
         c.x0 = x0;
@@ -689,7 +691,7 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
 #pragma unroll
             for (int j = 0; j < P::NOUT; ++j) {
                 *reinterpret_cast<float4*>(a.out[j] + at) = make_float4(o[0][j], o[1][j], o[2][j], o[3][j]);
-                if (P::checked(j) && a.rec[j] != nullptr) {
+                if (P::checked(j) && a.rec[j] != nullptr && own) {
                     const float bb[4] = {b[0][j], b[1][j], b[2][j], b[3][j]};
                     const float oo[4] = {o[0][j], o[1][j], o[2][j], o[3][j]};
                     fe_out_row4(acc[j], bb, oo, range);
@@ -698,7 +700,7 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         }
 #pragma unroll
         for (int j = 0; j < P::NOUT; ++j) {
-            if (P::checked(j) && a.rec[j] != nullptr && fe_out_plane(acc[j], a.lo[j], a.hi[j], range)) {
+            if (P::checked(j) && a.rec[j] != nullptr && own && fe_out_plane(acc[j], a.lo[j], a.hi[j], range)) {
                 // Read this lane's cells of the plane back (its own stores, through L2) and tally the bad ones.
 #pragma unroll
                 for (int r = 0; r < P::R; ++r) {
@@ -761,7 +763,7 @@ __device__ __forceinline__ void fe_plain_pass(const FePassArgs& a)
 #pragma unroll
         for (int j = 0; j < P::NOUT; ++j) {
             a.out[j][at] = o[j];
-            if (P::checked(j) && a.rec[j] != nullptr) {
+            if (P::checked(j) && a.rec[j] != nullptr && z >= a.own_z0 && z < a.own_z1) {
                 fe_out_cell(acc[j], b[j], o[j], a.lo[j], a.hi[j], static_cast<unsigned>(at), range, fails[j]);
             }
         }

@@ -70,6 +70,13 @@ class fe_heston_option(ctypes.Structure):
                 ("sigma", _c.c_float), ("rho", _c.c_float), ("r", _c.c_float)]
 
 
+class fe_group_totals(ctypes.Structure):
+    """Mirror of ``fe_group_totals`` (include/fe.h)."""
+
+    _fields_ = [("step", _c.c_longlong), ("term", _c.c_int), ("group", _c.c_int), ("substeps", _c.c_int), ("reserved", _c.c_int),
+                ("before", _c.c_double), ("after", _c.c_double), ("scale", _c.c_double)]
+
+
 class fe_step_info(ctypes.Structure):
     _fields_ = [("violations", _c.c_int), ("launches", _c.c_int), ("gpu_ms", _c.c_double)]
 
@@ -129,6 +136,11 @@ SIGNATURES = {
     "fe_law_fetch_device": (_i, [_p, _i, _p]),
     "fe_law_field_device_ptr": (_i, [_p, _i, _c.POINTER(_p)]),
     "fe_law_mark_edited": (_i, [_p, _i]),
+    "fe_law_set_owned_z": (_i, [_p, _i, _i]),
+    "fe_law_mark_halo": (_i, [_p, _i]),
+    "fe_law_set_external_conservation": (_i, [_p, _i]),
+    "fe_law_take_totals": (_i, [_p, _c.POINTER(fe_group_totals), _i, _c.POINTER(_i)]),
+    "fe_law_plan_z_reach": (_i, [_c.c_char_p, _i, _i, _i, _c.c_double, _c.POINTER(_i), _c.POINTER(_i)]),
     "fe_law_step": (_i, [_p, _d, _i, _c.POINTER(fe_step_info)]),
     "fe_law_derive": (_i, [_p]),
     "fe_law_check_every": (_i, [_p, _i]),

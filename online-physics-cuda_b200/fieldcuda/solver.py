@@ -190,6 +190,28 @@ class Solver:
         _lib.check(self._lib.fe_law_digest(self._h, ctypes.byref(d)))
         return d.value
 
+    # ---- one slab of a lattice split along z over ranks (fieldcuda.slabs) ---------------------------------------------
+    def set_owned_z(self, z0, z1):
+        """Contracts cover planes [z0, z1) of this handle only; the rest are halo planes another rank owns."""
+        _lib.check(self._lib.fe_law_set_owned_z(self._h, int(z0), int(z1)))
+
+    def mark_halo(self, field):
+        """The field's halo planes were written in place (on this solver's stream): its bounds are forgotten."""
+        _lib.check(self._lib.fe_law_mark_halo(self._h, self._id(field)))
+
+    def set_external_conservation(self, on):
+        """Checked steps log each conserves group's totals (take_totals) instead of judging them."""
+        _lib.check(self._lib.fe_law_set_external_conservation(self._h, 1 if on else 0))
+
+    def take_totals(self, room=4096):
+        """The logged group totals since the last call, oldest first: dicts of step, term, group, substeps, before,
+        after, scale."""
+        buf = (_lib.fe_group_totals * room)()
+        n = ctypes.c_int()
+        _lib.check(self._lib.fe_law_take_totals(self._h, buf, room, ctypes.byref(n)))
+        return [{"step": e.step, "term": e.term, "group": e.group, "substeps": e.substeps, "before": e.before, "after": e.after,
+                 "scale": e.scale} for e in buf[:n.value]]
+
     def time_gather(self, term=0, launches=10):
         ms = ctypes.c_float()
         _lib.check(self._lib.fe_law_time_gather(self._h, term, launches, ctypes.byref(ms)))
@@ -208,6 +230,13 @@ def ir_listing(law_text):
 def cuda_source(law_text, nx, ny, nz, h):
     """The generated CUDA translation unit (lawc --cuda)."""
     return _lib.text_call("fe_law_source", law_text.encode(), nx, ny, nz, float(h))
+
+
+def plan_z_reach(law_text, nx, ny, nz, h):
+    """(planes along z one step reads beyond a cell, reduces over the lattice, solves along z) for the planned law."""
+    reach, flags = ctypes.c_int(), ctypes.c_int()
+    _lib.check(_lib.lib().fe_law_plan_z_reach(law_text.encode(), nx, ny, nz, float(h), ctypes.byref(reach), ctypes.byref(flags)))
+    return reach.value, bool(flags.value & 1), bool(flags.value & 2)
 
 
 def compile_check(law_text, nx, ny, nz, h):
