@@ -627,6 +627,15 @@ private:
         }
         f << "extern \"C\" __global__ void __launch_bounds__(256) " << L.plain_kernel << "(const __grid_constant__ FePassArgs a) { fe_plain_pass<"
           << ns << "::P>(a); }\n";
+        // A pass with contracts also comes in a variant for a slab of a split lattice (halo planes left out of them).
+        if (std::any_of(L.checked_fields.begin(), L.checked_fields.end(), [](int f) { return f >= 0; })) {
+            if (L.slab) {
+                f << "extern \"C\" __global__ void __launch_bounds__(256) " << L.kernel << "_halo(const __grid_constant__ FePassArgs a) { fe_slab_pass<"
+                  << ns << "::P, true>(a); }\n";
+            }
+            f << "extern \"C\" __global__ void __launch_bounds__(256) " << L.plain_kernel << "_halo(const __grid_constant__ FePassArgs a) { fe_plain_pass<"
+              << ns << "::P, true>(a); }\n";
+        }
         out_ << f.str();
         return true;
     }

@@ -289,6 +289,10 @@ bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* r
         break;
     }
     a.blocks = static_cast<int>(gx * gy * gz);
+    if (L.kind == gen::Launch::Pass && (own_z0_ > 0 || own_z1_ < nz_) &&
+        std::any_of(L.checked_fields.begin(), L.checked_fields.end(), [](int f) { return f >= 0; })) {
+        name += "_halo";
+    }
     if (static_cast<std::size_t>(a.blocks) * 4 * FE_MAX_OUT > partial_doubles_) {
         why = "internal: too few partial sums for a launch";
         return false;

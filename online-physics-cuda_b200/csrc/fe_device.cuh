@@ -283,8 +283,9 @@ __device__ __forceinline__ void fe_out_init(FeOutAcc& a)
     a.changed = 0u;
 }
 
-// Four consecutive cells: their values before the pass (for the change flag) and after it.
-__device__ __forceinline__ void fe_out_row4(FeOutAcc& a, const float* before, const float* after, bool range)
+// Four consecutive cells: their values before the pass (for the change flag) and after it. `mask` is all ones on an owned
+// plane and zero on a halo plane, whose sums the plane's end drops.
+__device__ __forceinline__ void fe_out_row4(FeOutAcc& a, const float* before, const float* after, bool range, unsigned mask)
 {
     a.pa += (after[0] + after[1]) + (after[2] + after[3]);
     a.paa += (fabsf(after[0]) + fabsf(after[1])) + (fabsf(after[2]) + fabsf(after[3]));
@@ -292,8 +293,9 @@ __device__ __forceinline__ void fe_out_row4(FeOutAcc& a, const float* before, co
         a.lo = fminf(a.lo, fminf(fminf(after[0], after[1]), fminf(after[2], after[3])));
         a.hi = fmaxf(a.hi, fmaxf(fmaxf(after[0], after[1]), fmaxf(after[2], after[3])));
     }
-    a.changed |= ((__float_as_uint(before[0]) ^ __float_as_uint(after[0])) | (__float_as_uint(before[1]) ^ __float_as_uint(after[1])) |
-                     (__float_as_uint(before[2]) ^ __float_as_uint(after[2])) | (__float_as_uint(before[3]) ^ __float_as_uint(after[3]))) != 0u
+    a.changed |= (((__float_as_uint(before[0]) ^ __float_as_uint(after[0])) | (__float_as_uint(before[1]) ^ __float_as_uint(after[1])) |
+                      (__float_as_uint(before[2]) ^ __float_as_uint(after[2])) | (__float_as_uint(before[3]) ^ __float_as_uint(after[3]))) &
+                     mask) != 0u
         ? 1u : 0u;
 }
 
@@ -572,8 +574,9 @@ __device__ __forceinline__ void fe_pass_contracts(FeOutAcc* acc, double* scratch
 
 // The TMA z-marching pass: a CTA owns a 128 x TY column and marches a chunk of z-planes; every source's plane (with its
 // halo) comes into a ring of NST stages by one TMA load each, NST - 2 RZ - 1 planes ahead; one mbarrier a stage counts
-// the bytes of all sources. A lane computes 4 consecutive cells on R rows and stores them as float4.
-template <class P>
+// the bytes of all sources. A lane computes 4 consecutive cells on R rows and stores them as float4. HALO: the handle
+// holds halo planes another rank owns (a lattice split in z-slabs), left out of the contracts.
+template <class P, bool HALO = false>
 __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
 {
     extern __shared__ __align__(128) float fe_sm[];
@@ -652,7 +655,10 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
     // stages from it, the clamped ones at the lattice's z ends recompute them.
     int sz = zb - zlo;
     for (int z = zb; z < ze && !failed; ++z) {
-        const bool own = z >= a.own_z0 && z < a.own_z1;
+        // Halo planes (another rank's) are computed like the rest; their contributions to the contracts are dropped.
+        const bool own = !HALO || (z >= a.own_z0 && z < a.own_z1);
+        const bool range_here = range && own;
+        const unsigned own_mask = own ? 0xffffffffu : 0u;
         FeSlabCtx<P> c;
         c.sm = fe_sm;
         c.x0 = x0;
@@ -691,16 +697,19 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
 #pragma unroll
             for (int j = 0; j < P::NOUT; ++j) {
                 *reinterpret_cast<float4*>(a.out[j] + at) = make_float4(o[0][j], o[1][j], o[2][j], o[3][j]);
-                if (P::checked(j) && a.rec[j] != nullptr && own) {
+                if (P::checked(j) && a.rec[j] != nullptr) {
                     const float bb[4] = {b[0][j], b[1][j], b[2][j], b[3][j]};
                     const float oo[4] = {o[0][j], o[1][j], o[2][j], o[3][j]};
-                    fe_out_row4(acc[j], bb, oo, range);
+                    fe_out_row4(acc[j], bb, oo, range_here, own_mask);
                 }
             }
         }
 #pragma unroll
         for (int j = 0; j < P::NOUT; ++j) {
-            if (P::checked(j) && a.rec[j] != nullptr && own && fe_out_plane(acc[j], a.lo[j], a.hi[j], range)) {
+            if (!own) {
+                acc[j].pa = 0.f;
+                acc[j].paa = 0.f;
+            } else if (P::checked(j) && a.rec[j] != nullptr && fe_out_plane(acc[j], a.lo[j], a.hi[j], range)) {
                 // Read this lane's cells of the plane back (its own stores, through L2) and tally the bad ones.
 #pragma unroll
                 for (int r = 0; r < P::R; ++r) {
@@ -736,7 +745,7 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
 }
 
 // The plain pass: a thread a (x, y) column marching a chunk of z-planes, reads through the read-only path.
-template <class P>
+template <class P, bool HALO = false>
 __device__ __forceinline__ void fe_plain_pass(const FePassArgs& a)
 {
     __shared__ double scratch[4 * 8];
@@ -763,7 +772,7 @@ __device__ __forceinline__ void fe_plain_pass(const FePassArgs& a)
 #pragma unroll
         for (int j = 0; j < P::NOUT; ++j) {
             a.out[j][at] = o[j];
-            if (P::checked(j) && a.rec[j] != nullptr && z >= a.own_z0 && z < a.own_z1) {
+            if (P::checked(j) && a.rec[j] != nullptr && (!HALO || (z >= a.own_z0 && z < a.own_z1))) {
                 fe_out_cell(acc[j], b[j], o[j], a.lo[j], a.hi[j], static_cast<unsigned>(at), range, fails[j]);
             }
         }
