@@ -61,7 +61,7 @@ Radius axis_radius(const Inst& in)
 bool supported_cell_op(Op op)
 {
     switch (op) {
-    case Op::Distance: case Op::Poisson: case Op::Mlp: case Op::Flux: case Op::LDiffuse: case Op::Local:
+    case Op::Mlp: case Op::Flux: case Op::LDiffuse: case Op::Local:
         return false;
     default:
         return true;
@@ -79,6 +79,7 @@ public:
     {
         plan_.slot_of.assign(m_.insts.size(), -1);
         plan_.uniform_of.assign(m_.insts.size(), -1);
+        plan_.aux_of.assign(m_.insts.size(), -1);
         plan_.pingpong.assign(law_.fields.size(), 0);
         if (!allocate(why)) return false;
         out_ << device_prelude() << "\n";
@@ -143,7 +144,26 @@ private:
             case Op::MaxOf: case Op::MinOf: case Op::SumOf:
                 plan_.uniform_of[static_cast<std::size_t>(id)] = plan_.uniforms++;
                 break;
-            case Op::Distance: case Op::Poisson: case Op::Mlp: case Op::Flux: case Op::LDiffuse:
+            case Op::Distance:
+                // The answer, then seeds inside and outside, two scratch passes, squared distances to inside and
+                // outside (CudaSolver.cpp:394-418). The seeds start unlike any seed, so the first look solves.
+                plan_.slot_of[static_cast<std::size_t>(id)] = plan_.slots;
+                plan_.aux_of[static_cast<std::size_t>(id)] = plan_.slots + 1;
+                plan_.slot_fill.emplace_back(plan_.slots + 1, 0xffffffffu);
+                plan_.slots += 7;
+                flag_of_[id] = plan_.flags++;
+                break;
+            case Op::Poisson:
+                // The answer (warm-started from zero), the source as last solved (starting unlike any source), and
+                // the other half of the Jacobi ping-pong (CudaSolver.cpp:420-434).
+                plan_.slot_of[static_cast<std::size_t>(id)] = plan_.slots;
+                plan_.aux_of[static_cast<std::size_t>(id)] = plan_.slots + 1;
+                plan_.slot_fill.emplace_back(plan_.slots, 0u);
+                plan_.slot_fill.emplace_back(plan_.slots + 1, 0xffffffffu);
+                plan_.slots += 3;
+                flag_of_[id] = plan_.flags++;
+                break;
+            case Op::Mlp: case Op::Flux: case Op::LDiffuse:
                 why = std::string("this backend does not run '") + law::op_name(in.op) + "' stages yet";
                 return false;
             default:
@@ -708,6 +728,37 @@ private:
         return true;
     }
 
+    // A distance or poisson op: the seed pass (its argument at every cell, clamped reads) against what was last
+    // solved; the engine runs the fixed solve kernels after it.
+    void emit_solve(const std::string& tag, int id, Launch& L)
+    {
+        const Inst& in = at(id);
+        PassBuild pb;
+        walk(pb, in.args[0], Radius{}, false);
+        std::ostringstream f;
+        const std::string ns = "fe_" + tag;
+        f << "namespace " << ns << " {\n";
+        emit_functions(f, pb, {in.args[0]}, false);
+        L.kind = in.op == Op::Distance ? Launch::Distance : Launch::Poisson;
+        L.sources = pb.sources;
+        L.slab = false;
+        const int slot = plan_.slot_of[static_cast<std::size_t>(id)];
+        L.aux = plan_.aux_of[static_cast<std::size_t>(id)];
+        L.flag = flag_of_.at(id);
+        L.iterations = in.iterations;
+        L.outs = {Buf{Buf::Slot, slot}};
+        L.checked_fields = {-1};
+        emit_traits(f, pb, L, 0, {});
+        f << "    template <class C> static __device__ __forceinline__ float value(const C& c, int x, int y, int z) { constexpr bool IN = false; return "
+          << v(in.args[0]) << "; }\n"
+          << "    template <bool IN, class C> static __device__ __forceinline__ void cell(const C&, int, int, int, float*, float*) {}\n"
+          << "};\n}\n";
+        L.kernel = "fe_seed_" + tag;
+        f << "extern \"C\" __global__ void __launch_bounds__(256) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_seed_pass<" << ns
+          << "::P, " << (in.op == Op::Distance ? 1 : 0) << ">(a); }\n";
+        out_ << f.str();
+    }
+
     bool emit_reduce(const std::string& tag, int id, Launch& L)
     {
         const Inst& in = at(id);
@@ -762,6 +813,8 @@ private:
                 Launch L;
                 if (in.op == Op::Tridiag) {
                     if (!emit_tridiag(tag + "x" + std::to_string(n++), s, L, why)) return false;
+                } else if (in.op == Op::Distance || in.op == Op::Poisson) {
+                    emit_solve(tag + "d" + std::to_string(n++), s, L);
                 } else {
                     if (!emit_reduce(tag + "r" + std::to_string(n++), s, L)) return false;
                 }
@@ -841,6 +894,7 @@ private:
     int nx_, ny_, nz_;
     double h_;
     Plan& plan_;
+    std::map<int, int> flag_of_; // distance / poisson inst -> its change flag
     std::ostringstream out_;
 };
 

@@ -27,7 +27,7 @@ struct Source {
 };
 
 struct Launch {
-    enum Kind : unsigned char { Pass, TridiagX, TridiagYZ, Reduce } kind = Pass;
+    enum Kind : unsigned char { Pass, TridiagX, TridiagYZ, Reduce, Distance, Poisson } kind = Pass;
     std::string kernel;       // the slab (TMA) kernel, or the only one
     std::string plain_kernel; // the plain-load twin of a Pass
     std::vector<Source> sources;
@@ -40,6 +40,11 @@ struct Launch {
     int uniform = -1;         // Reduce: the uniform it writes
     int axis = 0;
     bool slab = true;         // the TMA variant is usable
+    // Distance / Poisson: the kernel is the seed pass (the argument against what was last solved, a flag when it
+    // changed); `aux` the first of the op's own slots, `flag` its word, `iterations` Poisson's sweeps.
+    int aux = -1;
+    int flag = -1;
+    int iterations = 0;
 };
 
 struct ProgramPlan {
@@ -56,6 +61,9 @@ struct Plan {
     int uniforms = 0;
     std::vector<int> slot_of;     // per inst: its stored slot (stored stages, tridiag answers), or -1
     std::vector<int> uniform_of;  // per inst: reductions' uniform, or -1
+    std::vector<int> aux_of;      // per inst: a distance's or poisson's own slots (after its answer), or -1
+    int flags = 0;                // change flags of the distance and poisson ops
+    std::vector<std::pair<int, unsigned>> slot_fill; // slots to fill at creation with a bit pattern
     std::vector<char> pingpong;   // per field: has a next buffer
     std::vector<ProgramPlan> terms, learned, derives;
     std::string source;           // the translation unit

@@ -45,6 +45,7 @@ Engine::~Engine()
     if (records_ != nullptr) cudaFree(records_);
     if (partials_ != nullptr) cudaFree(partials_);
     if (counts_ != nullptr) cudaFree(counts_);
+    if (flags_ != nullptr) cudaFree(flags_);
     if (ev0_ != nullptr) cudaEventDestroy(ev0_);
     if (ev1_ != nullptr) cudaEventDestroy(ev1_);
     if (stream_ != nullptr) cudaStreamDestroy(stream_);
@@ -127,6 +128,14 @@ bool Engine::create(const std::vector<law::Source>& sources, int nx, int ny, int
     for (float* s : slot_) {
         if (!cuda_ok(cudaMemsetAsync(s, 0, cells_ * sizeof(float), stream_), "memset", why)) return false;
     }
+    // What distance and poisson compare their input with starts unlike any input: the first look solves.
+    for (const auto& [slot, bits] : plan_.slot_fill) {
+        if (bits == 0u) continue;
+        float v = 0.0f;
+        std::memcpy(&v, &bits, sizeof(v));
+        if (!cuda_ok(launch_fill(slot_[static_cast<std::size_t>(slot)], cells_, v, sms_, stream_), "fill", why)) return false;
+    }
+    if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&flags_), std::max(1, plan_.flags) * sizeof(unsigned)), "cudaMalloc (flags)", why)) return false;
 
     // Contract records: one per checked output of every program, per step, in a ring.
     records_per_step_ = 0;
@@ -218,8 +227,54 @@ int Engine::zchunk_for(const gen::Launch& L, bool slab) const
     return std::max(1, zchunk);
 }
 
+bool Engine::launch_solve(const gen::Launch& L, float dt, std::string& why)
+{
+    FePassArgs a;
+    std::memset(&a, 0, sizeof(a));
+    for (std::size_t k = 0; k < L.sources.size(); ++k) {
+        float* p = nullptr;
+        if (!buffer(L.sources[k].buf, p)) {
+            why = "internal: a pass reads a buffer that does not exist";
+            return false;
+        }
+        a.src[k] = p;
+    }
+    const int answer = L.outs[0].id;
+    unsigned* flag = flags_ + L.flag;
+    a.out[0] = slot_[static_cast<std::size_t>(L.aux)];
+    a.out[1] = L.kind == gen::Launch::Distance ? slot_[static_cast<std::size_t>(L.aux + 1)] : nullptr;
+    a.flag = flag;
+    a.err = counts_ + FE_MAX_OUT;
+    a.dt = dt;
+    a.own_z0 = 0;
+    a.own_z1 = nz_;
+    if (!cuda_ok(cudaMemsetAsync(flag, 0, sizeof(unsigned), stream_), "flag", why)) return false;
+    const unsigned gx = static_cast<unsigned>(std::min<std::size_t>((cells_ + 255) / 256, static_cast<std::size_t>(sms_) * 4));
+    a.blocks = static_cast<int>(gx);
+    CUfunction fn = function(L.kernel, 0, why);
+    if (fn == nullptr) return false;
+    void* params[] = {&a};
+    ++launches_;
+    if (!cu_ok(driver().launchKernel(fn, gx, 1, 1, 256, 1, 1, 0, reinterpret_cast<CUstream>(stream_), params, nullptr), ("launch " + L.kernel).c_str(), why)) {
+        return false;
+    }
+    const float hf = static_cast<float>(h_);
+    if (L.kind == gen::Launch::Distance) {
+        float* slots[7];
+        slots[0] = slot_[static_cast<std::size_t>(answer)];
+        for (int k = 0; k < 6; ++k) slots[1 + k] = slot_[static_cast<std::size_t>(L.aux + k)];
+        launches_ += 7;
+        return cuda_ok(launch_distance_solve(slots, nx_, ny_, nz_, hf, flag, sms_, stream_), "distance", why);
+    }
+    launches_ += L.iterations + (L.iterations % 2);
+    return cuda_ok(launch_poisson_solve(slot_[static_cast<std::size_t>(answer)], slot_[static_cast<std::size_t>(L.aux + 1)],
+                       slot_[static_cast<std::size_t>(L.aux)], L.iterations, nx_, ny_, nz_, hf, flag, sms_, stream_),
+        "poisson", why);
+}
+
 bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* recs, std::string& why, const FeCheck* const* carry)
 {
+    if (L.kind == gen::Launch::Distance || L.kind == gen::Launch::Poisson) return launch_solve(L, dt, why);
     FePassArgs a;
     std::memset(&a, 0, sizeof(a));
     const bool slab = L.kind == gen::Launch::Pass && L.slab;
@@ -287,6 +342,9 @@ bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* r
         block = 256;
         gx = static_cast<unsigned>(std::min<std::size_t>((cells_ + 255) / 256, static_cast<std::size_t>(sms_) * 4));
         break;
+    case gen::Launch::Distance:
+    case gen::Launch::Poisson:
+        break; // launch_solve, above
     }
     a.blocks = static_cast<int>(gx * gy * gz);
     if (L.kind == gen::Launch::Pass && (own_z0_ > 0 || own_z1_ < nz_) &&
@@ -387,7 +445,7 @@ void plan_z_reach(const gen::Plan& plan, int& reach, bool& reductions, bool& z_s
     z_solves = false;
     auto count = [&](const gen::Launch& L) {
         if (L.kind == gen::Launch::Pass) reach += L.rz;
-        if (L.kind == gen::Launch::Reduce) reductions = true;
+        if (L.kind == gen::Launch::Reduce || L.kind == gen::Launch::Distance || L.kind == gen::Launch::Poisson) reductions = true;
         if (L.kind == gen::Launch::TridiagYZ && L.axis == 2) z_solves = true;
     };
     for (const auto* progs : {&plan.terms, &plan.derives}) {

@@ -124,6 +124,7 @@ private:
 
     bool launch(const gen::Launch& L, float dt, int flags, FeCheck* const* recs, std::string& why, const FeCheck* const* carry = nullptr);
     bool conserved_by(int term, int field) const;
+    bool launch_solve(const gen::Launch& L, float dt, std::string& why);
     bool buffer(const gen::Buf& b, float*& out) const;
     bool map_for(const float* base, int bx, int by, FeTensorMap& out, std::string& why);
     CUfunction function(const std::string& name, unsigned smem, std::string& why);
@@ -161,6 +162,7 @@ private:
     double* partials_ = nullptr;
     std::size_t partial_doubles_ = 0;
     unsigned* counts_ = nullptr; // FE_MAX_OUT counters, then the error word
+    unsigned* flags_ = nullptr;  // change flags of the distance and poisson ops
     std::vector<PendingStep> pending_;
     std::vector<double> param_host_;
     bool params_dirty_ = true;

@@ -53,6 +53,7 @@ struct FePassArgs {
     float hi[FE_MAX_OUT];
     double* partials;          // [FE_MAX_OUT][blocks][4]
     unsigned* count;           // [FE_MAX_OUT] blocks finished
+    unsigned* flag;            // a distance's or poisson's change flag (its seed pass sets it)
     unsigned* err;
     float dt;
     int flags;                 // FE_PASS_AFTER | FE_PASS_RANGE
@@ -778,6 +779,33 @@ __device__ __forceinline__ void fe_plain_pass(const FePassArgs& a)
         }
     }
     fe_pass_contracts<P>(acc, scratch, fails, a);
+}
+
+// The seed pass of a distance (DIST) or poisson op: its argument at every cell against what was last solved, kept in
+// out[0]; when any cell differs, the flag is raised and the solve kernels after it run. distance: the seed is 0 where the
+// argument is at least 0.5 (solid) and 1e30 elsewhere, out[1] the complement; poisson: out[0] the source itself.
+template <class P, int DIST>
+__device__ __forceinline__ void fe_seed_pass(const FePassArgs& a)
+{
+    FePlainCtx<P> c;
+    c.src = a.src;
+    c.dt = a.dt;
+    const fe_u64 cells = static_cast<fe_u64>(P::NX) * P::NY * P::NZ;
+    const fe_u64 stride = static_cast<fe_u64>(gridDim.x) * blockDim.x;
+    bool changed = false;
+    for (fe_u64 i = blockIdx.x * static_cast<fe_u64>(blockDim.x) + threadIdx.x; i < cells; i += stride) {
+        const int x = static_cast<int>(i % P::NX);
+        const int y = static_cast<int>((i / P::NX) % P::NY);
+        const int z = static_cast<int>(i / (static_cast<fe_u64>(P::NX) * P::NY));
+        const float v = P::value(c, x, y, z);
+        const float seed = DIST ? (v >= 0.5f ? 0.f : 1e30f) : v;
+        if (__float_as_uint(a.out[0][i]) != __float_as_uint(seed)) {
+            a.out[0][i] = seed;
+            if (DIST) a.out[1][i] = seed == 0.f ? 1e30f : 0.f;
+            changed = true;
+        }
+    }
+    if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) atomicOr(a.flag, 1u);
 }
 
 // A deterministic reduction of one expression over the lattice (maxof / minof / sumof): a fixed assignment of cells to

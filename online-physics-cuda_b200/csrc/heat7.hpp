@@ -1,4 +1,4 @@
-// Host-side interface of the hand-written kernels in heat7.cu and totals.cu.
+// Host-side interface of the hand-written kernels in heat7.cu, totals.cu and field_solves.cu.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -43,6 +43,12 @@ cudaError_t launch_fill(float* p, size_t n, float v, int sms, cudaStream_t strea
 constexpr int kTotalsBlocks = 1184;
 cudaError_t launch_totals(const float* v, size_t n, FeCheck* rec, double* partials, unsigned* count, cudaStream_t stream);
 cudaError_t launch_copy(const float* a, float* b, size_t n, int sms, cudaStream_t stream);
+// The solves of distance and poisson (field_solves.cu), after their seed pass; each kernel returns at once unless *flag.
+// distance slots: 0 the answer, 1 seeds inside, 2 seeds outside, 3 and 4 scratch, 5 and 6 squared distances. Launches:
+// 7 for distance, `iterations` (+1 when odd) for poisson.
+cudaError_t launch_distance_solve(float* const slots[7], int nx, int ny, int nz, float h, const unsigned* flag, int sms, cudaStream_t stream);
+cudaError_t launch_poisson_solve(float* answer, float* other, const float* source, int iterations, int nx, int ny, int nz, float h,
+    const unsigned* flag, int sms, cudaStream_t stream);
 int heat7_tma_rows(int variant);
 int heat7_tma_blocks(int variant, int nx, int ny, int nz, int zchunk);
 int heat7_plain_blocks(int nx, int ny, int nz, int zchunk);

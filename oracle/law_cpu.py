@@ -53,8 +53,9 @@ def _uniform(v):
 class Evaluator:
     """One gather: every value of the pre-state computed once (the reference's epoch sharing)."""
 
-    def __init__(self, law, fields, zero, h, dt):
+    def __init__(self, law, fields, zero, h, dt, keep=None):
         self.law = law
+        self.keep = keep if keep is not None else {}  # what distance and poisson keep between evaluations
         self.fields = fields
         self.zero = zero
         self.h = h
@@ -172,7 +173,97 @@ class Evaluator:
             return float(flat.max() if op == "maxof" else flat.min())
         if op in ("fall", "spread", "topple"):
             return getattr(self, "_" + op)(*(self(x) for x in a))
+        if op == "distance":
+            return self._distance(i, self._arr(self(a[0])).astype(F32))
+        if op == "poisson":
+            return self._poisson(i, self._arr(self(a[0])).astype(F32), int(ins["iterations"]))
         raise NotImplementedError(f"the oracle does not restate '{op}'")
+
+    # ---- the whole-lattice ops (Law.cpp:1042-1098, 1139-1181) ---------------------------------------------------------
+    @staticmethod
+    def _squared_distance(feature):
+        """Exact squared distance (in cells) of every cell to the nearest cell of `feature`, inf without one: a 1-D
+        pass along x, then y, then z, each the least over the axis of (what the previous pass found) + r^2
+        (Law.cpp:489-525 computes the same numbers with a lower-envelope pass)."""
+        d = np.where(feature, 0.0, np.inf)
+        for axis in (2, 1, 0):
+            n = d.shape[axis]
+            if n == 1:
+                continue
+            best = d.copy()
+            for r in range(1, n):
+                rr = float(r * r)
+                lo = np.full_like(d, np.inf)
+                hi = np.full_like(d, np.inf)
+                sl_dst = [slice(None)] * 3
+                sl_src = [slice(None)] * 3
+                sl_dst[axis], sl_src[axis] = slice(r, None), slice(None, n - r)
+                lo[tuple(sl_dst)] = d[tuple(sl_src)]
+                sl_dst[axis], sl_src[axis] = slice(None, n - r), slice(r, None)
+                hi[tuple(sl_dst)] = d[tuple(sl_src)]
+                best = np.minimum(best, np.minimum(lo, hi) + rr)
+            d = best
+        return d
+
+    def _distance(self, i, a):
+        """Signed distance in metres to the surface of {a >= 0.5} (negative inside), the surface half a cell from the
+        last solid cell's centre, beyond the lattice open. Recomputed only when a's bits change (Law.cpp:1042-1098)."""
+        key = ("distance", i)
+        k = a.tobytes()
+        if key in self.keep and self.keep[key][0] == k:
+            return self.keep[key][1]
+        nz, ny, nx = self.shape
+        h = self.h
+        far = (nx + ny + nz) * h
+        inside = a >= 0.5
+        any_in, any_out = bool(inside.any()), bool((~inside).any())
+        to_in = self._squared_distance(inside) if any_in else None
+        to_out = self._squared_distance(~inside) if any_out else None
+        z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        border = np.full(self.shape, np.inf)
+        for q, n in ((x, nx), (y, ny), (z, nz)):
+            if n > 1:
+                border = np.minimum(border, np.minimum(q + 1, n - q).astype(np.float64))
+        out_cells = np.minimum(np.sqrt(to_out) if any_out else far / h, border)
+        d_in = -(out_cells - 0.5) * h
+        d_out = (np.sqrt(to_in) - 0.5) * h if any_in else np.full(self.shape, far)
+        out = np.where(inside, d_in, d_out).astype(F32)
+        self.keep[key] = (k, out)
+        return out
+
+    def _poisson(self, i, s, iterations):
+        """`iterations` Jacobi sweeps of lap(phi) = s (phi = 0 beyond the lattice), warm-started from the last answer;
+        skipped while s keeps its bits (Law.cpp:1139-1181)."""
+        key = ("poisson", i)
+        k = s.tobytes()
+        phi = self.keep.get(key, (None, np.zeros(self.shape, F32)))
+        if phi[0] == k:
+            return phi[1]
+        phi = phi[1]
+        nz, ny, nx = self.shape
+        axes = sum(1 for n in (nx, ny, nz) if n > 1)
+        denom = 2.0 * max(axes, 1)
+        h = self.h
+        src = s.astype(np.float64)
+        for _ in range(iterations):
+            p = phi.astype(np.float64)
+            total = np.zeros(self.shape)
+            for axis, n in ((2, nx), (1, ny), (0, nz)):
+                if n < 2:
+                    continue
+                lo = np.zeros(self.shape)
+                hi = np.zeros(self.shape)
+                sl_dst = [slice(None)] * 3
+                sl_src = [slice(None)] * 3
+                sl_dst[axis], sl_src[axis] = slice(1, None), slice(None, -1)
+                lo[tuple(sl_dst)] = p[tuple(sl_src)]
+                sl_dst[axis], sl_src[axis] = slice(None, -1), slice(1, None)
+                hi[tuple(sl_dst)] = p[tuple(sl_src)]
+                total = total + lo
+                total = total + hi
+            phi = ((total - h * h * src) / denom).astype(F32)
+        self.keep[key] = (k, phi)
+        return phi
 
     # ---- stencils (Law.cpp:947-985) ----------------------------------------------------------------------------------
     def _neighbours(self, v):
@@ -442,6 +533,7 @@ class Solver:
             self.fields[d["name"]] = np.full(shape, F32(d["init"]), dtype=F32)
         self.violations = []
         self.substeps = [1] * len(law.terms)
+        self.keep = {}  # distance's and poisson's answers and the inputs they were solved for
 
     def _zero(self):
         return {k: not np.any(v != 0) for k, v in self.fields.items()}
@@ -451,7 +543,7 @@ class Solver:
         for t, term in enumerate(self.law.terms):
             self._integrate(t, term, dt)
         for d in self.law.derives:
-            ev = Evaluator(self.law, self.fields, self._zero(), self.h, 0.0)
+            ev = Evaluator(self.law, self.fields, self._zero(), self.h, 0.0, self.keep)
             target = self.law.fields[d["equations"][0][0]]
             v = ev(d["equations"][0][1])
             old = self.fields[target].astype(np.float64) if d["accumulate"] else 0.0
@@ -462,7 +554,7 @@ class Solver:
         self.substeps[t] = 1
         count = 1
         if term["max_dt"] >= 0:
-            ev = Evaluator(law, self.fields, self._zero(), self.h, 0.0)
+            ev = Evaluator(law, self.fields, self._zero(), self.h, 0.0, self.keep)
             limit = ev(term["max_dt"])
             if _is_scalar(limit) and limit > 0.0 and math.isfinite(limit) and dt > limit:
                 wanted = math.ceil(dt / limit)
@@ -476,7 +568,7 @@ class Solver:
         before = None
         touched = False
         for _ in range(count):
-            ev = Evaluator(law, self.fields, self._zero(), self.h, sub_dt)
+            ev = Evaluator(law, self.fields, self._zero(), self.h, sub_dt, self.keep)
             deltas = []
             for target, value in term["equations"]:
                 v = ev(value)

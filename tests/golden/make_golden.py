@@ -104,6 +104,18 @@ def cases():
     out.append(dict(name="multifield43", law="multifield43.law", shape=n, h=1.0 / 20, dt=0.1 * (1.0 / 20) ** 2, steps=3,
                     fields={f"f{i}": rngm.uniform(-1, 1, n).astype(np.float32) for i in range(6)}))
     out.append(dict(name="heston_explicit", law="heston_explicit.law", shape=(3, 16, 32), h=h, dt=0.01, steps=3, fields=f))
+    # distance and poisson: the per-op starting state of the reference's CUDA gate (a smooth A, B solid in a pattern),
+    # then both ops with a drifting source.
+    n = (9, 14, 20)
+    z, y, x = np.meshgrid(np.arange(9), np.arange(14), np.arange(20), indexing="ij")
+    A = (0.5 + 0.4 * np.sin(0.7 * x + 0.3 * y) * np.cos(0.5 * z)).astype(np.float32)
+    B = ((x + 2 * y + 3 * z) % 7 < 3).astype(np.float32)
+    for name in ("op_distance", "op_poisson"):
+        out.append(dict(name=name, law=name + ".law", shape=n, h=0.5, dt=0.02, steps=4, fields={"A": A, "B": B}))
+    n = (10, 12, 16)
+    rngf = np.random.default_rng(21)
+    out.append(dict(name="ops_fields", law="ops_fields.law", shape=n, h=0.5, dt=0.05, steps=4,
+                    fields={"b": (rngf.uniform(0, 1, n) < 0.3).astype(np.float32)}))
     return out
 
 

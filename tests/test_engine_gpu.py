@@ -14,7 +14,8 @@ pytestmark = pytest.mark.gpu
 GOLDEN = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
 # Relative tolerance against the reference's CPU solver (which computes every op in double and stores float): the
 # reference's own gate holds one op to 2e-5 and a whole law to 1e-4 (src/tests/cuda_parity_smoke.cpp:114-117, 159-160).
-TOLERANCE = {"heat_24": 1e-6, "ops_stencil": 2e-5, "ops_matter": 2e-5, "cn_64": 2e-5, "implicit_yz": 2e-5}
+TOLERANCE = {"heat_24": 1e-6, "ops_stencil": 2e-5, "ops_matter": 2e-5, "cn_64": 2e-5, "implicit_yz": 2e-5, "op_distance": 2e-5,
+             "op_poisson": 2e-5}
 
 
 def load(path):

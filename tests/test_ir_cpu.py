@@ -59,6 +59,9 @@ def test_law_errors_name_the_line():
 
 def test_unsupported_ops_are_refused_not_faked():
     from fieldcuda import _lib, solver
+    law = "field T init 290 range 0 6000\nnet ld in 5 hidden 8 out 4 act tanh file none\nterm t\n  d T = ldiffuse(ld, 0.8, T)\n"
     with pytest.raises(_lib.FeError) as e:
-        solver.compile_check("field s init 0\nfield q init 0\nterm t\n  d q = distance(s) - q\n", 8, 8, 8, 1.0)
-    assert e.value.code == _lib.FE_EUNSUP
+        solver.compile_check(law, 8, 8, 8, 1.0)
+    assert e.value.code == _lib.FE_EUNSUP and "ldiffuse" in str(e.value)
+    # distance and poisson are run (their solves after a seed pass), not refused
+    solver.compile_check("field s init 0\nfield q init 0\nterm t\n  d q = distance(s) - q + poisson(s, 5)\n", 8, 8, 8, 1.0)
