@@ -161,6 +161,34 @@ def ir_fixtures(lawc):
         print("ir", name)
 
 
+def scene_fixtures(lawc):
+    """lawc --scene on tests/scenes/*.scene (from the repository root, where the scenes' law paths point): the state the
+    scene makes (step_0, after refresh_derived) and the state after the steps, for the CLI's parity tests."""
+    out_dir = os.path.join(HERE, "scene")
+    os.makedirs(out_dir, exist_ok=True)
+    for name, steps, dt in (("ops", 3, 0.05),):
+        work = tempfile.mkdtemp(prefix="fe_scene_")
+        try:
+            dump = os.path.join(work, "dump")
+            js = os.path.join(work, "t.json")
+            subprocess.run([lawc, "--scene", os.path.join("tests", "scenes", name + ".scene"), "--steps", str(steps), "--dt", repr(dt),
+                            "--dump", dump, "--json", js], check=True, capture_output=True, cwd=ROOT,
+                           env=dict(os.environ, OMP_NUM_THREADS="4"))
+            meta_dump = json.load(open(os.path.join(dump, "step_0", "meta.json")))
+            shape = (meta_dump["nz"], meta_dump["ny"], meta_dump["nx"])
+            arrays = {}
+            for k in (0, steps):
+                for f in meta_dump["fields"]:
+                    arrays[f"step{k}_{f}"] = np.fromfile(os.path.join(dump, f"step_{k}", f + ".bin"), np.float32).reshape(shape)
+            timing = json.load(open(js))
+            meta = dict(scene=name + ".scene", steps=steps, dt=dt, fields=meta_dump["fields"], substeps=timing["substeps"],
+                        violations=timing["violations"], made_by="the reference's lawc --scene (its OpenMP CPU Solver)")
+            np.savez_compressed(os.path.join(out_dir, name + ".npz"), meta=json.dumps(meta), **arrays)
+            print("scene", name)
+        finally:
+            shutil.rmtree(work, ignore_errors=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--lawc", default=os.path.join(ROOT, "oracle", "_ref", "lawc"))
@@ -169,6 +197,7 @@ def main():
     if not os.path.exists(args.lawc):
         sys.exit(f"no reference solver at {args.lawc}: build it with `make -C oracle ref`")
     ir_fixtures(args.lawc)
+    scene_fixtures(args.lawc)
     for case in cases():
         if args.only and case["name"] not in args.only.split(","):
             continue
