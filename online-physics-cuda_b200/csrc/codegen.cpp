@@ -54,6 +54,8 @@ Radius axis_radius(const Inst& in)
     case Op::Gz: case Op::GzT: return {0, 0, 1};
     case Op::Fall: return {0, 0, 1};
     case Op::Spread: return {1, 1, 0};
+    case Op::Flux: return {1, 1, 1};
+    case Op::LDiffuse: return {2, 2, 2};
     default: return {};
     }
 }
@@ -61,7 +63,7 @@ Radius axis_radius(const Inst& in)
 bool supported_cell_op(Op op)
 {
     switch (op) {
-    case Op::Mlp: case Op::Flux: case Op::LDiffuse: case Op::Local:
+    case Op::Local:
         return false;
     default:
         return true;
@@ -87,6 +89,12 @@ public:
         out_ << "__device__ float FE_U[" << std::max(plan_.uniforms, 1) << "];\n";
         out_ << "constexpr int NX = " << nx_ << ", NY = " << ny_ << ", NZ = " << nz_ << ";\n";
         out_ << "constexpr float FE_H = " << literal(h_) << ";\n";
+        {
+            char hd[48];
+            std::snprintf(hd, sizeof(hd), "%.17g", h_);
+            out_ << "constexpr double FE_HD = " << hd << ";\n";
+        }
+        emit_nets();
         out_ << R"(__device__ __forceinline__ int fe_ex(int v) { return v < 0 ? 0 : (v >= NX ? NX - 1 : v); }
 __device__ __forceinline__ int fe_ey(int v) { return v < 0 ? 0 : (v >= NY ? NY - 1 : v); }
 __device__ __forceinline__ int fe_ez(int v) { return v < 0 ? 0 : (v >= NZ ? NZ - 1 : v); }
@@ -163,9 +171,6 @@ private:
                 plan_.slots += 3;
                 flag_of_[id] = plan_.flags++;
                 break;
-            case Op::Mlp: case Op::Flux: case Op::LDiffuse:
-                why = std::string("this backend does not run '") + law::op_name(in.op) + "' stages yet";
-                return false;
             default:
                 plan_.slot_of[static_cast<std::size_t>(id)] = plan_.slots++;
                 break;
@@ -420,6 +425,87 @@ private:
               << "    }\n    return o; }\n";
             break;
         }
+        case Op::Mlp: {
+            // mlp(NET, a...): the net at the cell, its first output (Law.cpp:1298-1333).
+            const law::NetDecl& net = law_.nets[static_cast<std::size_t>(in.index)];
+            f << " { float xin[" << in.args.size() << "];\n";
+            for (std::size_t k = 0; k < in.args.size(); ++k) f << "    xin[" << k << "] = " << a(k) << ";\n";
+            f << "    float yout[" << net.sizes.back() << "]; fe_net" << in.index << "(xin, yout); return yout[0]; }\n";
+            break;
+        }
+        case Op::Flux: {
+            // flux(NET, F, a..., lo, hi): across each face (i below, j above) the net sees both sides both ways round;
+            // half the difference, limited, is what moves from i to j; a cell gains its lower faces' and loses its upper
+            // faces', over h (Law.cpp:1335-1389, 691-706). Both cells of a face compute it the same way: antisymmetric.
+            const law::NetDecl& net = law_.nets[static_cast<std::size_t>(in.index)];
+            const std::size_t m = in.args.size() - 2;
+            const double lo = at(in.args[m]).number;
+            const double hi = at(in.args[m + 1]).number;
+            const std::string n = std::to_string(id);
+            char bounds[96];
+            std::snprintf(bounds, sizeof(bounds), "%.17g, %.17g", lo, hi);
+            f << ";\n";
+            f << "template <bool IN, class C> __device__ __forceinline__ float face" << n
+              << "(const C& c, int ix, int iy, int iz, int jx, int jy, int jz) {\n    float xij[" << 2 * m << "], xji[" << 2 * m << "];\n";
+            for (std::size_t k = 0; k < m; ++k) {
+                f << "    { const float vi = " << a(k, "ix", "iy", "iz") << "; const float vj = " << a(k, "jx", "jy", "jz") << "; xij[" << k
+                  << "] = vi; xij[" << m + k << "] = vj; xji[" << k << "] = vj; xji[" << m + k << "] = vi; }\n";
+            }
+            f << "    float y[" << net.sizes.back() << "]; fe_net" << in.index << "(xij, y); const float gij = y[0]; fe_net" << in.index
+              << "(xji, y); const float gji = y[0];\n"
+              << "    return fe_limit_face(0.5f * (gij - gji), xij[0], xij[" << m << "], " << bounds << ", c.dt); }\n";
+            f << "template <bool IN, class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)"
+              << " { float o = 0.f;\n"
+              << "    if (IN || x > 0) o += face" << n << "<IN>(c, x - 1, y, z, x, y, z);\n"
+              << "    if (IN || x + 1 < NX) o -= face" << n << "<IN>(c, x, y, z, x + 1, y, z);\n"
+              << "    if (IN || y > 0) o += face" << n << "<IN>(c, x, y - 1, z, x, y, z);\n"
+              << "    if (IN || y + 1 < NY) o -= face" << n << "<IN>(c, x, y, z, x, y + 1, z);\n"
+              << "    if (IN || z > 0) o += face" << n << "<IN>(c, x, y, z - 1, x, y, z);\n"
+              << "    if (IN || z + 1 < NZ) o -= face" << n << "<IN>(c, x, y, z, x, y, z + 1);\n"
+              << "    return o / FE_H; }\n";
+            break;
+        }
+        case Op::LDiffuse: {
+            // ldiffuse(NET, k, F): the flux through a face from the window F[i-1] F[i] | F[j] F[j+1] (edge cells repeat),
+            // with weights the net gives around the classical [0 -1 1 0]; each way round, half the difference
+            // (Law.cpp:1391-1438, 708-738). k's face value is the harmonic mean, in double like the reference.
+            const std::string n = std::to_string(id);
+            f << ";\n";
+            f << "__device__ __forceinline__ float lraw" << n << "(const float* w, float kf, float dt) {\n"
+              << "    const float centre = 0.5f * (w[1] + w[2]); float spread = 1e-6f;\n"
+              << "#pragma unroll\n    for (int q = 0; q < 4; ++q) spread = fmaxf(spread, fabsf(w[q] - centre));\n"
+              << "    float xin[5];\n#pragma unroll\n    for (int q = 0; q < 4; ++q) xin[q] = (w[q] - centre) / spread;\n"
+              << "    xin[4] = kf * dt / (FE_H * FE_H);\n"
+              << "    float yw[4]; fe_net" << in.index << "(xin, yw);\n"
+              << "    const float mean = 0.25f * (yw[0] + yw[1] + yw[2] + yw[3]);\n"
+              << "    const float base[4] = {0.f, -1.f, 1.f, 0.f}; float acc = 0.f;\n"
+              << "#pragma unroll\n    for (int q = 0; q < 4; ++q) acc += (base[q] + (yw[q] - mean)) * w[q];\n"
+              << "    return -kf / FE_H * acc; }\n";
+            // The face between cell i = (x, y, z) and its +AX neighbour j.
+            f << "template <bool IN, int AX, class C> __device__ __forceinline__ float ldface" << n << "(const C& c, int x, int y, int z) {\n"
+              << "    const int jx = x + (AX == 0), jy = y + (AX == 1), jz = z + (AX == 2);\n"
+              << "    const int q = AX == 0 ? x : (AX == 1 ? y : z); const int count = AX == 0 ? NX : (AX == 1 ? NY : NZ);\n"
+              << "    const int mx = (IN || q > 0) ? x - (AX == 0) : x, my = (IN || q > 0) ? y - (AX == 1) : y, mz = (IN || q > 0) ? z - (AX == 2) : z;\n"
+              << "    const int px = (IN || q + 2 < count) ? jx + (AX == 0) : jx, py = (IN || q + 2 < count) ? jy + (AX == 1) : jy,"
+              << " pz = (IN || q + 2 < count) ? jz + (AX == 2) : jz;\n"
+              << "    const float w[4] = {" << a(1, "mx", "my", "mz") << ", " << a(1, "x", "y", "z") << ", " << a(1, "jx", "jy", "jz") << ", "
+              << a(1, "px", "py", "pz") << "};\n"
+              << "    const double ka = " << a(0, "x", "y", "z") << ", kb = " << a(0, "jx", "jy", "jz") << ";\n"
+              << "    const float kf = static_cast<float>((ka + kb) > 0.0 ? 2.0 * ka * kb / (ka + kb) : 0.0);\n"
+              << "    const float mirror[4] = {w[3], w[2], w[1], w[0]};\n"
+              << "    const float ij = lraw" << n << "(w, kf, c.dt); const float ji = lraw" << n << "(mirror, kf, c.dt);\n"
+              << "    return 0.5f * (ij - ji); }\n";
+            f << "template <bool IN, class C> __device__ __forceinline__ float " << name << "(const C& c, int x, int y, int z)"
+              << " { float o = 0.f;\n"
+              << "    if (IN || x > 0) o += ldface" << n << "<IN, 0>(c, x - 1, y, z);\n"
+              << "    if (IN || x + 1 < NX) o -= ldface" << n << "<IN, 0>(c, x, y, z);\n"
+              << "    if (IN || y > 0) o += ldface" << n << "<IN, 1>(c, x, y - 1, z);\n"
+              << "    if (IN || y + 1 < NY) o -= ldface" << n << "<IN, 1>(c, x, y, z);\n"
+              << "    if (IN || z > 0) o += ldface" << n << "<IN, 2>(c, x, y, z - 1);\n"
+              << "    if (IN || z + 1 < NZ) o -= ldface" << n << "<IN, 2>(c, x, y, z);\n"
+              << "    return o / FE_H; }\n";
+            break;
+        }
         case Op::Tridiag: case Op::MaxOf: case Op::MinOf: case Op::SumOf:
             // Only as a body: the stage kernels evaluate their arguments directly.
             simple("0.f");
@@ -428,6 +514,62 @@ private:
             simple("0.f");
             break;
         }
+    }
+
+    // The law's nets: their parameters in one module array, FE_NET (the engine writes plan.net_blob there), and a
+    // forward function a net, fe_net<k>(in, out), in the reference's order (Net.cpp:93-153): inputs shifted and scaled,
+    // then per layer out[o] = bias[o] + sum_i W[o][i] x[i] in i order, the activation on every layer but the last, the
+    // outputs times out_scale. fp32, no FMA contraction, like the reference's CPU nets.
+    void emit_nets()
+    {
+        std::ostringstream f;
+        for (std::size_t k = 0; k < law_.nets.size(); ++k) {
+            const law::NetDecl& net = law_.nets[k];
+            const std::size_t w0 = plan_.net_blob.size();
+            plan_.net_blob.insert(plan_.net_blob.end(), net.weights.begin(), net.weights.end());
+            const std::size_t sh = plan_.net_blob.size();
+            plan_.net_blob.insert(plan_.net_blob.end(), net.in_shift.begin(), net.in_shift.end());
+            const std::size_t sc = plan_.net_blob.size();
+            plan_.net_blob.insert(plan_.net_blob.end(), net.in_scale.begin(), net.in_scale.end());
+            const std::size_t os = plan_.net_blob.size();
+            plan_.net_blob.push_back(net.out_scale);
+            const std::string act = net.act == "tanh" ? "tanhf(v)" : net.act == "relu" ? "(v > 0.f ? v : 0.f)" : net.act == "silu" ? "v / (1.f + expf(-v))" : "v";
+            f << "__device__ __forceinline__ float fe_act" << k << "(float v) { return " << act << "; }\n";
+            f << "__device__ __forceinline__ void fe_net" << k << "(const float* in, float* out) {\n";
+            const int n0 = net.sizes.front();
+            f << "    float h0[" << n0 << "];\n#pragma unroll\n    for (int i = 0; i < " << n0 << "; ++i) h0[i] = (in[i] - FE_NET[" << sh << " + i]) * FE_NET[" << sc
+              << " + i];\n";
+            for (int l = 0; l < net.layers(); ++l) {
+                const int ni = net.sizes[static_cast<std::size_t>(l)];
+                const int no = net.sizes[static_cast<std::size_t>(l) + 1];
+                const std::size_t wl = w0 + net.weight_offset(l);
+                const bool last = l + 1 == net.layers();
+                f << "    float h" << l + 1 << "[" << no << "];\n#pragma unroll\n    for (int o = 0; o < " << no << "; ++o) {\n"
+                  << "        float acc = FE_NET[" << wl + static_cast<std::size_t>(ni) * no << " + o];\n#pragma unroll\n        for (int i = 0; i < " << ni
+                  << "; ++i) acc += FE_NET[" << wl << " + o * " << ni << " + i] * h" << l << "[i];\n"
+                  << "        h" << l + 1 << "[o] = " << (last ? "acc" : "fe_act" + std::to_string(k) + "(acc)") << ";\n    }\n";
+            }
+            f << "#pragma unroll\n    for (int o = 0; o < " << net.sizes.back() << "; ++o) out[o] = h" << net.layers() << "[o] * FE_NET[" << os << "];\n}\n";
+        }
+        out_ << "__device__ float FE_NET[" << std::max<std::size_t>(1, plan_.net_blob.size()) << "];\n";
+        out_ << R"(// The flux limiter of flux(): the same on both sides of a face, so the flux stays antisymmetric; within one step of dt
+// no cell goes below the moved field's least or above its most (Law.cpp:672-689).
+__device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, double lo, double hi, float dt)
+{
+    if (!(dt > 0.f)) return r;
+    const float per = static_cast<float>(0.999 * FE_HD / (6.0 * static_cast<double>(dt)));
+    const bool has_lo = lo > -1e29, has_hi = hi < 1e29;
+    if (r > 0.f) {
+        if (has_lo) r = fminf(r, fmaxf(0.f, (fi - static_cast<float>(lo)) * per));
+        if (has_hi) r = fminf(r, fmaxf(0.f, (static_cast<float>(hi) - fj) * per));
+    } else if (r < 0.f) {
+        if (has_lo) r = fmaxf(r, -fmaxf(0.f, (fj - static_cast<float>(lo)) * per));
+        if (has_hi) r = fmaxf(r, -fmaxf(0.f, (static_cast<float>(hi) - fi) * per));
+    }
+    return r;
+}
+)";
+        out_ << f.str();
     }
 
     // The pass traits: lattice, tile, sources' layout, outputs' checks.

@@ -64,6 +64,7 @@ struct Plan {
     std::vector<int> aux_of;      // per inst: a distance's or poisson's own slots (after its answer), or -1
     int flags = 0;                // change flags of the distance and poisson ops
     std::vector<std::pair<int, unsigned>> slot_fill; // slots to fill at creation with a bit pattern
+    std::vector<float> net_blob;  // the nets' parameters as the module's FE_NET holds them (weights, shift, scale, out scale)
     std::vector<char> pingpong;   // per field: has a next buffer
     std::vector<ProgramPlan> terms, learned, derives;
     std::string source;           // the translation unit

@@ -89,6 +89,19 @@ bool Engine::create(const std::vector<law::Source>& sources, int nx, int ny, int
     std::size_t bytes = 0;
     if (!cu_ok(d.moduleGetGlobal(&params_, &bytes, module_, "FE_P"), "FE_P", why)) return false;
     if (!cu_ok(d.moduleGetGlobal(&uniforms_, &bytes, module_, "FE_U"), "FE_U", why)) return false;
+    if (!plan_.net_blob.empty()) {
+        // The nets' parameters (their files', or the untrained start) into the module's FE_NET.
+        CUdeviceptr nets = 0;
+        if (!cu_ok(d.moduleGetGlobal(&nets, &bytes, module_, "FE_NET"), "FE_NET", why)) return false;
+        if (bytes < plan_.net_blob.size() * sizeof(float)) {
+            why = "internal: FE_NET is smaller than the nets' parameters";
+            return false;
+        }
+        if (!cuda_ok(cudaMemcpy(reinterpret_cast<void*>(nets), plan_.net_blob.data(), plan_.net_blob.size() * sizeof(float), cudaMemcpyHostToDevice),
+                "nets", why)) {
+            return false;
+        }
+    }
     if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate", why)) return false;
     if (!cuda_ok(cudaEventCreate(&ev0_), "cudaEventCreate", why) || !cuda_ok(cudaEventCreate(&ev1_), "cudaEventCreate", why)) return false;
 

@@ -406,7 +406,7 @@ std::string to_json(const Module& m, const law::Law& law)
         json_string(out, net.file);
         out << ",\"sizes\":";
         json_ints(out, net.sizes);
-        out << ",\"act\":\"" << net.act << "\",\"half\":" << (net.half ? "true" : "false") << ",\"loaded\":false}";
+        out << ",\"act\":\"" << net.act << "\",\"half\":" << (net.half ? "true" : "false") << ",\"loaded\":" << (net.loaded ? "true" : "false") << "}";
     }
     out << "],\"insts\":[";
     for (std::size_t i = 0; i < m.insts.size(); ++i) {

@@ -577,7 +577,8 @@ Law compile(const std::vector<Source>& sources, std::vector<std::string>& errors
                 }
                 section = tok.text;
                 if (section == "act") {
-                    bad = t[i].kind != Token::Name || !(t[i].text == "tanh" || t[i].text == "relu" || t[i].text == "silu");
+                    bad = t[i].kind != Token::Name ||
+                        !(t[i].text == "tanh" || t[i].text == "relu" || t[i].text == "silu" || t[i].text == "linear");
                     net.act = t[i].text;
                     ++i;
                 } else if (section == "half") {
@@ -602,6 +603,13 @@ Law compile(const std::vector<Source>& sources, std::vector<std::string>& errors
             net.sizes.push_back(in);
             net.sizes.insert(net.sizes.end(), hidden.begin(), hidden.end());
             net.sizes.push_back(out);
+            // Untrained unless its file is there (a missing file is not an error: the net starts at 0).
+            init_net(net);
+            std::string why;
+            if (!load_net(net, why) && why.rfind("no weights at", 0) != 0) {
+                errors.push_back(line.where + ": " + why);
+                continue;
+            }
             law.nets.push_back(net);
             continue;
         }

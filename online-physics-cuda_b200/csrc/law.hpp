@@ -70,7 +70,21 @@ struct NetDecl {
     std::string act;
     bool half = false;
     std::string file;
+    // Its parameters (Net.hpp's layout): per layer the out x in weights row by row, then the out biases; the inputs'
+    // shift and scale; the output scale. Untrained (no file) it starts from init_net; `loaded` once a file was read.
+    std::vector<float> weights, in_shift, in_scale;
+    float out_scale = 1.0f;
+    bool loaded = false;
+    [[nodiscard]] int layers() const { return static_cast<int>(sizes.size()) - 1; }
+    [[nodiscard]] std::size_t weight_offset(int layer) const;
+    [[nodiscard]] std::size_t parameter_count() const { return weight_offset(layers()); }
 };
+
+// The starting weights of a net (Net.cpp:241-262): hidden layers uniform in +-sqrt(6 / (in + out)) from a hash of the
+// net's name, layer and index; the last layer and every bias zero, so an untrained net outputs 0.
+void init_net(NetDecl& net, std::uint64_t seed = 0);
+// Reads the net's weight file (Net.cpp:264-333's text format). False with "no weights at ..." when there is no file.
+bool load_net(NetDecl& net, std::string& error);
 
 struct Law {
     std::vector<Node> nodes;

@@ -11,6 +11,7 @@ arrays shaped (nz, ny, nx). Pinned bit for bit against the reference's own solve
 """
 import json
 import math
+import os
 
 import numpy as np
 
@@ -29,12 +30,109 @@ class Law:
         self.terms = ir["terms"]
         self.derives = ir["derives"]
         self._cost = [None] * len(self.insts)
+        self.nets = [Net(n) for n in ir.get("nets", [])]
 
     def cost(self, i):
         """Subtree size, everything inlined (the reference's node cost, Law.cpp:1518-1521)."""
         if self._cost[i] is None:
             self._cost[i] = 1 + sum(self.cost(a) for a in self.insts[i]["args"])
         return self._cost[i]
+
+
+class Net:
+    """A law's net with its parameters: its weight file if there is one (relative to the working directory, as for the
+    reference), else the untrained start (src/field/nn/Net.cpp:241-333)."""
+
+    def __init__(self, decl):
+        self.name = decl["name"]
+        self.sizes = list(decl["sizes"])
+        self.act = decl["act"]
+        self.out_scale = np.float32(1.0)
+        self.shift = np.zeros(self.sizes[0], F32)
+        self.scale = np.ones(self.sizes[0], F32)
+        self.weights = self._init()
+        if os.path.exists(decl["file"]):
+            self._load(decl["file"])
+
+    def offset(self, layer):
+        return sum((self.sizes[l] + 1) * self.sizes[l + 1] for l in range(layer))
+
+    def _init(self, seed=0):
+        mask = (1 << 64) - 1
+
+        def fin(h):
+            h ^= h >> 33
+            h = (h * 0xFF51AFD7ED558CCD) & mask
+            h ^= h >> 33
+            h = (h * 0xC4CEB9FE1A85EC53) & mask
+            h ^= h >> 33
+            return h
+        w = np.zeros(self.offset(len(self.sizes) - 1), F32)
+        h = 1469598103934665603 ^ seed
+        for c in self.name.encode():
+            h = ((h ^ c) * 1099511628211) & mask
+        for l in range(len(self.sizes) - 2):
+            ni, no = self.sizes[l], self.sizes[l + 1]
+            limit = np.sqrt(F32(6.0) / F32(ni + no), dtype=F32)
+            base = self.offset(l)
+            for k in range(ni * no):
+                r = fin((h + l * 0x9E3779B97F4A7C15 + k) & mask)
+                u = F32((r >> 11) * (1.0 / 9007199254740992.0))
+                w[base + k] = (F32(2.0) * u - F32(1.0)) * limit
+        return w
+
+    def _load(self, path):
+        words = open(path).read().split()
+        section, i = None, 0
+        sizes, shift, scale, weights = [], [], [], []
+        while i < len(words):
+            w = words[i]
+            i += 1
+            if w == "net":
+                i += 1
+            elif w == "act":
+                i += 1
+                section = None
+            elif w == "out_scale":
+                self.out_scale = F32(float(words[i]))
+                i += 1
+                section = None
+            elif w in ("sizes", "in_shift", "in_scale", "weights"):
+                section = w
+            else:
+                {"sizes": sizes, "in_shift": shift, "in_scale": scale, "weights": weights}[section].append(float(w))
+        assert [int(s) for s in sizes] == self.sizes, path
+        self.weights = np.array(weights, F32)
+        self.shift = np.zeros(self.sizes[0], F32)
+        self.shift[:len(shift)] = shift
+        self.scale = np.ones(self.sizes[0], F32)
+        self.scale[:len(scale)] = scale
+
+    def _activate(self, v):
+        if self.act == "tanh":
+            return np.tanh(v.astype(np.float64)).astype(F32)
+        if self.act == "relu":
+            return np.where(v > 0, v, F32(0.0)).astype(F32)
+        if self.act == "silu":
+            return (v / (F32(1.0) + np.exp(-v.astype(np.float64)).astype(F32))).astype(F32)
+        return v
+
+    def forward(self, x):
+        """x: (cells, inputs) float32 -> (cells, outputs) float32, in the reference's float order."""
+        h = ((x.astype(F32) - self.shift) * self.scale).astype(F32)
+        layers = len(self.sizes) - 1
+        for l in range(layers):
+            ni, no = self.sizes[l], self.sizes[l + 1]
+            w = self.weights[self.offset(l):self.offset(l) + ni * no].reshape(no, ni)
+            b = self.weights[self.offset(l) + ni * no:self.offset(l) + ni * no + no]
+            out = np.empty((h.shape[0], no), F32)
+            for o in range(no):
+                acc = np.full(h.shape[0], b[o], F32)
+                for i in range(ni):
+                    acc = (acc + (w[o, i] * h[:, i]).astype(F32)).astype(F32)
+                out[:, o] = acc
+            h = self._activate(out) if l + 1 < layers else out
+        return (h * self.out_scale).astype(F32)
 
 
 def _settle(a):
@@ -173,11 +271,124 @@ class Evaluator:
             return float(flat.max() if op == "maxof" else flat.min())
         if op in ("fall", "spread", "topple"):
             return getattr(self, "_" + op)(*(self(x) for x in a))
+        if op == "mlp":
+            net = self.law.nets[ins["index"]]
+            xs = [self(x) for x in a]
+            if all(_is_scalar(v) for v in xs):
+                return float(net.forward(np.array([[F32(v) for v in xs]], F32))[0, 0])
+            x = np.stack([self._arr(v).astype(F32).reshape(-1) for v in xs], axis=1)
+            return _settle(net.forward(x)[:, 0].reshape(self.shape))
+        if op == "flux":
+            return self._flux(self.law.nets[ins["index"]], [self(x) for x in a[:-2]], self.law.insts[a[-2]]["number"],
+                              self.law.insts[a[-1]]["number"])
+        if op == "ldiffuse":
+            return self._ldiffuse(self.law.nets[ins["index"]], self(a[0]), self(a[1]))
         if op == "distance":
             return self._distance(i, self._arr(self(a[0])).astype(F32))
         if op == "poisson":
             return self._poisson(i, self._arr(self(a[0])).astype(F32), int(ins["iterations"]))
         raise NotImplementedError(f"the oracle does not restate '{op}'")
+
+    # ---- the net ops' faces (Law.cpp:672-738, 1335-1438) -------------------------------------------------------------
+    def _faces_to_cells(self, wide):
+        """wide[0], [1], [2]: the flux from each cell through its +x, +y, +z face (0 where there is none); the cell's
+        gain over h."""
+        out = np.zeros(self.shape, F32)
+        for a, axis in enumerate((2, 1, 0)):  # x, y, z: each its lower face's in, then its upper face's out
+            lower = np.zeros(self.shape, F32)
+            sl_dst = [slice(None)] * 3
+            sl_src = [slice(None)] * 3
+            sl_dst[axis], sl_src[axis] = slice(1, None), slice(None, -1)
+            lower[tuple(sl_dst)] = wide[a][tuple(sl_src)]
+            out = (out + lower).astype(F32)
+            out = (out - wide[a]).astype(F32)
+        return _settle((out / F32(self.h)).astype(F32))
+
+    def _pairs(self, axis):
+        """Index arrays (i, j) of every face along an axis, i the lower cell."""
+        n = self.shape[axis]
+        idx = np.arange(int(np.prod(self.shape))).reshape(self.shape)
+        sl_i = [slice(None)] * 3
+        sl_j = [slice(None)] * 3
+        sl_i[axis], sl_j[axis] = slice(None, n - 1), slice(1, None)
+        return idx[tuple(sl_i)], idx[tuple(sl_j)], tuple(sl_i)
+
+    def _flux(self, net, vals, lo, hi):
+        if all(_uniform(v) for v in vals):
+            return 0.0
+        arrs = [self._arr(v).astype(F32).reshape(-1) for v in vals]
+        m = len(arrs)
+        dt = self.dt
+        per = F32(0.999 * self.h / (6.0 * dt)) if dt > 0 else None
+        wide = []
+        for axis in (2, 1, 0):
+            w = np.zeros(self.shape, F32)
+            i, j, sl = self._pairs(axis)
+            if i.size:
+                i, j = i.reshape(-1), j.reshape(-1)
+                xi = np.stack([a[i] for a in arrs], axis=1)
+                xj = np.stack([a[j] for a in arrs], axis=1)
+                gij = net.forward(np.concatenate([xi, xj], axis=1))[:, 0]
+                gji = net.forward(np.concatenate([xj, xi], axis=1))[:, 0]
+                r = (F32(0.5) * (gij - gji).astype(F32)).astype(F32)
+                if per is not None:
+                    fi, fj = xi[:, 0], xj[:, 0]
+                    pos, neg = r > 0, r < 0
+                    if lo > -1e29:
+                        r = np.where(pos, np.minimum(r, np.maximum(F32(0), ((fi - F32(lo)) * per).astype(F32))), r)
+                    if hi < 1e29:
+                        r = np.where(pos, np.minimum(r, np.maximum(F32(0), ((F32(hi) - fj) * per).astype(F32))), r)
+                    if lo > -1e29:
+                        r = np.where(neg, np.maximum(r, -np.maximum(F32(0), ((fj - F32(lo)) * per).astype(F32))), r)
+                    if hi < 1e29:
+                        r = np.where(neg, np.maximum(r, -np.maximum(F32(0), ((F32(hi) - fi) * per).astype(F32))), r)
+                w[sl] = r.astype(F32).reshape(w[sl].shape)
+            wide.append(w)
+        return self._faces_to_cells(wide)
+
+    def _ldiffuse(self, net, k, f):
+        if _uniform(f):
+            return 0.0
+        F = self._arr(f).astype(F32)
+        K = self._arr(k)
+        dt = F32(self.dt)
+        h = F32(self.h)
+        wide = []
+        for axis in (2, 1, 0):
+            n = self.shape[axis]
+            w = np.zeros(self.shape, F32)
+            if n > 1:
+                q = np.arange(n)
+                im = np.where(q > 0, q - 1, q)[:n - 1]
+                jp = np.where(q + 2 < n, q + 2, q + 1)[:n - 1]
+                take = lambda a, idx: np.take(a, idx, axis=axis)
+                win = [take(F, im), take(F, q[:n - 1]), take(F, q[1:]), take(F, jp)]
+                ka = take(K, q[:n - 1]).astype(np.float64)
+                kb = take(K, q[1:]).astype(np.float64)
+                s = ka + kb
+                kf = np.where(s > 0, 2.0 * ka * kb / np.where(s > 0, s, 1.0), 0.0).astype(F32)
+
+                def raw(wv):
+                    centre = (F32(0.5) * (wv[1] + wv[2]).astype(F32)).astype(F32)
+                    spread = np.full(centre.shape, F32(1e-6), F32)
+                    for a in range(4):
+                        spread = np.maximum(spread, np.abs((wv[a] - centre).astype(F32)))
+                    x = [((wv[a] - centre).astype(F32) / spread).astype(F32) for a in range(4)]
+                    x.append(((kf * dt).astype(F32) / (h * h)).astype(F32))
+                    y = net.forward(np.stack([v.reshape(-1) for v in x], axis=1))
+                    y = [y[:, a].reshape(centre.shape) for a in range(4)]
+                    mean = (F32(0.25) * ((((y[0] + y[1]).astype(F32) + y[2]).astype(F32) + y[3]).astype(F32))).astype(F32)
+                    acc = np.zeros(centre.shape, F32)
+                    for a, base in enumerate((0.0, -1.0, 1.0, 0.0)):
+                        acc = (acc + ((F32(base) + (y[a] - mean).astype(F32)).astype(F32) * wv[a]).astype(F32)).astype(F32)
+                    return ((-kf / h).astype(F32) * acc).astype(F32)
+                ij = raw(win)
+                ji = raw(win[::-1])
+                sl = [slice(None)] * 3
+                sl[axis] = slice(None, n - 1)
+                w[tuple(sl)] = (F32(0.5) * (ij - ji).astype(F32)).astype(F32)
+            wide.append(w)
+        return self._faces_to_cells(wide)
 
     # ---- the whole-lattice ops (Law.cpp:1042-1098, 1139-1181) ---------------------------------------------------------
     @staticmethod

@@ -112,6 +112,14 @@ def cases():
     B = ((x + 2 * y + 3 * z) % 7 < 3).astype(np.float32)
     for name in ("op_distance", "op_poisson"):
         out.append(dict(name=name, law=name + ".law", shape=n, h=0.5, dt=0.02, steps=4, fields={"A": A, "B": B}))
+    # The net ops (weights in tests/laws/nets/, read relative to the repository root like the reference's assets/nets).
+    rngn = np.random.default_rng(31)
+    for shape, tag in (((9, 14, 20), ""), ((4, 6, 136), "_wide")):
+        T = (290.0 + 900.0 * rngn.uniform(0, 1, shape) * (rngn.uniform(0, 1, shape) < 0.3)).astype(np.float32)
+        fuel = rngn.uniform(0, 1, shape).astype(np.float32)
+        out.append(dict(name="nets_mlp" + tag, law="nets_mlp.law", shape=shape, h=0.5, dt=0.02, steps=3, fields={"T": T, "fuel": fuel}))
+        out.append(dict(name="nets_flux" + tag, law="nets_flux.law", shape=shape, h=0.5, dt=0.02, steps=3, fields={"T": T, "fuel": fuel}))
+        out.append(dict(name="nets_ldiffuse" + tag, law="nets_ldiffuse.law", shape=shape, h=0.5, dt=0.02, steps=3, fields={"T": T}))
     n = (10, 12, 16)
     rngf = np.random.default_rng(21)
     out.append(dict(name="ops_fields", law="ops_fields.law", shape=n, h=0.5, dt=0.05, steps=4,
@@ -133,7 +141,7 @@ def run(case, lawc, work):
     js = os.path.join(work, "t.json")
     cmd = [lawc, "--scene", scene, "--init", init, "--steps", str(case["steps"]), "--dt", repr(case["dt"]), "--dump", dump,
            "--json", js]
-    res = subprocess.run(cmd, capture_output=True, text=True, env=dict(os.environ, OMP_NUM_THREADS="4"))
+    res = subprocess.run(cmd, capture_output=True, text=True, cwd=ROOT, env=dict(os.environ, OMP_NUM_THREADS="4"))
     if res.returncode != 0:
         raise RuntimeError(f"{case['name']}: lawc failed\n{res.stdout}\n{res.stderr}")
     meta_dump = json.load(open(os.path.join(dump, f"step_{case['steps']}", "meta.json")))
@@ -157,7 +165,7 @@ def ir_fixtures(lawc):
         if not name.endswith(".law"):
             continue
         out = os.path.join(out_dir, name[:-4] + ".json")
-        subprocess.run([lawc, "--ir-json", out, os.path.join(LAWS, name)], check=True, capture_output=True)
+        subprocess.run([lawc, "--ir-json", out, os.path.join(LAWS, name)], check=True, capture_output=True, cwd=ROOT)
         print("ir", name)
 
 

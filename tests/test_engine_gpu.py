@@ -28,6 +28,7 @@ def load(path):
 
 def run_case(meta, init, steps=None):
     from fieldcuda.solver import Solver
+    os.chdir(ROOT)  # net weight files (tests/laws/nets/) are read from the repository root
     nz, ny, nx = meta["shape"]
     s = Solver(open(os.path.join(ROOT, "tests", "laws", meta["law"])).read(), nx, ny, nz, meta["h"], meta["law"])
     for name, arr in init.items():

@@ -12,12 +12,11 @@ LAWS = sorted(glob.glob(os.path.join(ROOT, "tests", "laws", "*.law")))
 
 
 @pytest.mark.parametrize("law", LAWS, ids=lambda p: os.path.basename(p))
-def test_ir_json_matches_reference(law):
+def test_ir_json_matches_reference(law, monkeypatch):
     from fieldcuda import solver
+    monkeypatch.chdir(ROOT)  # a net's weight file path is relative to the working directory (loaded: true there)
     mine = json.loads(solver.ir_json(open(law).read()))
     ref = json.load(open(os.path.join(ROOT, "tests", "golden", "ir", os.path.basename(law)[:-4] + ".json")))
-    for n in ref["nets"]:
-        n["loaded"] = False  # weights files are the host's, not the IR's
     assert mine == ref
 
 
@@ -57,11 +56,15 @@ def test_law_errors_name_the_line():
         solver.ir_json("field T init 0 static\nterm t\n  d T = 1\n")  # writes a static field
 
 
-def test_unsupported_ops_are_refused_not_faked():
+def test_bad_net_files_are_refused_not_faked(monkeypatch):
     from fieldcuda import _lib, solver
-    law = "field T init 290 range 0 6000\nnet ld in 5 hidden 8 out 4 act tanh file none\nterm t\n  d T = ldiffuse(ld, 0.8, T)\n"
+    monkeypatch.chdir(ROOT)
+    # fx's file holds a 2-16-16-1 net: a law declaring another shape for it does not compile
+    law = "field T init 290 range 0 6000\nnet fx in 2 hidden 8 out 1 act tanh file tests/laws/nets/fx\nterm t\n  d T = mlp(fx, T, T)\n"
     with pytest.raises(_lib.FeError) as e:
         solver.compile_check(law, 8, 8, 8, 1.0)
-    assert e.value.code == _lib.FE_EUNSUP and "ldiffuse" in str(e.value)
-    # distance and poisson are run (their solves after a seed pass), not refused
+    assert e.value.code == _lib.FE_ELAW and "sizes" in str(e.value)
+    # distance, poisson and the net ops are run (not refused); a net without a file starts untrained
     solver.compile_check("field s init 0\nfield q init 0\nterm t\n  d q = distance(s) - q + poisson(s, 5)\n", 8, 8, 8, 1.0)
+    law = "field T init 290 range 0 6000\nnet ld in 5 hidden 8 out 4 act tanh file none\nterm t\n  d T = ldiffuse(ld, 0.8, T)\n"
+    solver.compile_check(law, 8, 8, 8, 1.0)

@@ -19,8 +19,9 @@ def load(path):
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=lambda p: os.path.basename(p)[:-4])
-def test_oracle_reproduces_reference_solver(path):
+def test_oracle_reproduces_reference_solver(path, monkeypatch):
     from oracle import law_cpu
+    monkeypatch.chdir(ROOT)  # net weight files are found from the repository root, as the fixtures were made
     meta, init, final = load(path)
     ir = json.load(open(os.path.join(ROOT, "tests", "golden", "ir", meta["law"][:-4] + ".json")))
     law = law_cpu.Law(ir)
@@ -30,10 +31,13 @@ def test_oracle_reproduces_reference_solver(path):
     for _ in range(meta["steps"]):
         s.step(meta["dt"])
     assert s.substeps == meta["substeps"]
+    # A net's tanh/exp come from numpy here and from the C library there: a net law is held to a few units in the last
+    # place, every other law to the bit.
+    ulps = 4 if meta["law"].startswith("nets_") else 0
     for name, want in final.items():
         got = s.fields[name]
-        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (
-            f"{meta['name']}:{name} differs by {np.abs(got.astype(np.float64) - want).max()}")
+        apart = np.abs(got.view(np.int32).astype(np.int64) - want.view(np.int32).astype(np.int64)).max()
+        assert apart <= ulps, f"{meta['name']}:{name} differs by {np.abs(got.astype(np.float64) - want).max()} ({apart} ulps)"
 
 
 def test_heat_restatement_matches_the_law_oracle():
