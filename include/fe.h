@@ -129,6 +129,7 @@ typedef struct fe_step_info {
     int violations;      /* violations now held (fe_law_violation) */
     int launches;        /* kernels the step launched */
     double gpu_ms;       /* the step's device time (0 when it did not wait for the card) */
+    int fallbacks;       /* learned schemes undone this step (a broken contract; the classical scheme ran) */
 } fe_step_info;
 
 typedef struct fe_field_info {
@@ -217,6 +218,12 @@ int fe_law_violation(const fe_law* law, int index, fe_violation* out);
 int fe_law_substeps(const fe_law* law, int term);
 /* Whether the term did nothing in the last step (its bounds said idle; TermProfile::idle). */
 int fe_law_term_idle(const fe_law* law, int term);
+/* Learned schemes under guard (Solver::set_learned, Solver.hpp; the guard Solver.cpp:314-336, CudaSolver.cpp:663-708):
+ * with `on`, a term with `learned` equations runs them first on a snapshot of what it writes, its contracts judged at
+ * once; a broken one undoes the step (never reported) and the classical equations run. fe_law_term_learned: 1 the
+ * term's learned scheme was kept in the last step, 2 it was undone, 0 the classical scheme ran alone, -1 no such term. */
+int fe_law_set_learned(fe_law* law, int on);
+int fe_law_term_learned(const fe_law* law, int term);
 /* FNV-1a over every field's bits in declaration order (FieldSet::digest, src/field/Grid.cpp:60-77). */
 int fe_law_digest(fe_law* law, uint64_t* out);
 /* The handle's stream (a cudaStream_t), for callers that order their own work after its steps. */

@@ -51,6 +51,7 @@ void fill_info(const fe_law* l, fe_step_info* info)
     info->violations = static_cast<int>(l->engine.violations().size());
     info->launches = l->engine.launches_last_step();
     info->gpu_ms = l->engine.gpu_ms_last_step();
+    info->fallbacks = l->engine.fallbacks_last_step();
 }
 
 } // namespace
@@ -366,6 +367,20 @@ int fe_law_violation(const fe_law* law, int index, fe_violation* out)
     out->step = v.step;
     std::strncpy(out->detail, v.detail.c_str(), sizeof(out->detail) - 1);
     return fe::ok();
+}
+
+int fe_law_set_learned(fe_law* law, int on)
+{
+    if (law == nullptr) return fe::fail(FE_EINVAL, "null handle");
+    law->engine.set_learned(on != 0);
+    return fe::ok();
+}
+
+int fe_law_term_learned(const fe_law* law, int term)
+{
+    if (law == nullptr || term < 0 || static_cast<size_t>(term) >= law->engine.term_profile().size()) return -1;
+    const fe::TermProfile& p = law->engine.term_profile()[static_cast<size_t>(term)];
+    return p.fell_back ? 2 : (p.learned ? 1 : 0);
 }
 
 int fe_law_substeps(const fe_law* law, int term)

@@ -46,6 +46,7 @@ Engine::~Engine()
     if (partials_ != nullptr) cudaFree(partials_);
     if (counts_ != nullptr) cudaFree(counts_);
     if (flags_ != nullptr) cudaFree(flags_);
+    if (snapshot_ != nullptr) cudaFree(snapshot_);
     if (ev0_ != nullptr) cudaEventDestroy(ev0_);
     if (ev1_ != nullptr) cudaEventDestroy(ev1_);
     if (stream_ != nullptr) cudaStreamDestroy(stream_);
@@ -797,8 +798,9 @@ bool Engine::step(double dt, bool respect_max_dt, std::string& why)
         }
     }
     cudaEventRecord(ev0_, stream_);
+    fallbacks_ = 0;
     for (std::size_t t = 0; t < mod_.terms.size(); ++t) {
-        if (!run_program(static_cast<int>(t), mod_.terms[t], plan_.terms[t], dt, respect_max_dt, check, pending, why)) return false;
+        if (!apply_term(static_cast<int>(t), dt, respect_max_dt, check, pending, why)) return false;
     }
     for (std::size_t d = 0; d < mod_.derives.size(); ++d) {
         const gen::ProgramPlan& pp = plan_.derives[d];
@@ -874,7 +876,83 @@ bool Engine::sync(std::string& why)
 }
 
 // The host's judgement of one step's records (CudaSolver.cpp:530-571; the tolerance is Solver.cpp:439-453's).
+bool Engine::apply_term(int t, double dt, bool respect, bool check, PendingStep& pending, std::string& why)
+{
+    const std::size_t ti = static_cast<std::size_t>(t);
+    const bool guarded = learned_ && ti < mod_.learned.size() && !mod_.learned[ti].equations.empty() && ti < plan_.learned.size() &&
+        !plan_.learned[ti].empty;
+    if (!guarded) return run_program(t, mod_.terms[ti], plan_.terms[ti], dt, respect, check, pending, why);
+    // GUARDED: what the term writes goes aside; the learned scheme runs with its contracts checked and judged now.
+    const ir::Program& lp = mod_.learned[ti];
+    std::vector<int> writes = lp.writes;
+    for (const int w : mod_.terms[ti].writes) {
+        if (std::find(writes.begin(), writes.end(), w) == writes.end()) writes.push_back(w);
+    }
+    if (snapshot_fields_ < writes.size()) {
+        if (snapshot_ != nullptr) cudaFree(snapshot_);
+        snapshot_ = nullptr;
+        snapshot_fields_ = 0;
+        if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&snapshot_), writes.size() * cells_ * sizeof(float)), "cudaMalloc (snapshot)", why)) return false;
+        snapshot_fields_ = writes.size();
+    }
+    for (std::size_t w = 0; w < writes.size(); ++w) {
+        if (!cuda_ok(cudaMemcpyAsync(snapshot_ + w * cells_, now_[static_cast<std::size_t>(writes[w])], cells_ * sizeof(float), cudaMemcpyDeviceToDevice,
+                         stream_),
+                "snapshot", why)) {
+            return false;
+        }
+    }
+    const std::vector<Bounds> bounds_before = bounds_;
+    const std::vector<char> zero_before = zero_;
+    const std::size_t mark = pending.refs.size();
+    // Its records start empty (on an unchecked step the slot was not cleared for it).
+    if (!cuda_ok(cudaMemsetAsync(records_ + static_cast<std::size_t>(pending.ring) * records_per_step_ + mark, 0,
+                     plan_.learned[ti].gather.outs.size() * sizeof(FeCheck), stream_),
+            "records", why)) {
+        return false;
+    }
+    if (!run_program(t, lp, plan_.learned[ti], dt, respect, true, pending, why)) return false;
+    std::vector<Violation> broken;
+    if (pending.refs.size() > mark) {
+        if (!cuda_ok(cudaStreamSynchronize(stream_), "guard", why)) return false;
+        PendingStep trial;
+        trial.step = pending.step;
+        trial.ring = pending.ring;
+        trial.refs.assign(pending.refs.begin() + static_cast<std::ptrdiff_t>(mark), pending.refs.end());
+        if (!judge_into(trial, broken, why)) return false;
+    }
+    TermProfile& tp = term_profile_[ti];
+    if (broken.empty()) {
+        tp.learned = !tp.idle;
+        if (!check) pending.refs.resize(mark); // an unchecked step keeps no records of it
+        return true;
+    }
+    // Undo it: the snapshot back, its records cleared, the bounds as they were; then the classical scheme.
+    for (std::size_t w = 0; w < writes.size(); ++w) {
+        const std::size_t f = static_cast<std::size_t>(writes[w]);
+        if (!cuda_ok(cudaMemcpyAsync(now_[f], snapshot_ + w * cells_, cells_ * sizeof(float), cudaMemcpyDeviceToDevice, stream_), "undo", why)) return false;
+        carry_[f] = Carry{};
+    }
+    const std::size_t used = pending.refs.size() - mark;
+    if (!cuda_ok(cudaMemsetAsync(records_ + static_cast<std::size_t>(pending.ring) * records_per_step_ + mark, 0, used * sizeof(FeCheck), stream_), "records",
+            why)) {
+        return false;
+    }
+    pending.refs.resize(mark);
+    bounds_ = bounds_before;
+    zero_ = zero_before;
+    ++fallbacks_;
+    if (!run_program(t, mod_.terms[ti], plan_.terms[ti], dt, respect, check, pending, why)) return false;
+    term_profile_[ti].fell_back = true;
+    return true;
+}
+
 bool Engine::judge(PendingStep& pending, std::string& why)
+{
+    return judge_into(pending, violations_, why);
+}
+
+bool Engine::judge_into(const PendingStep& pending, std::vector<Violation>& out, std::string& why)
 {
     if (pending.refs.empty()) return true;
     std::vector<FeCheck> recs(static_cast<std::size_t>(records_per_step_));
@@ -921,7 +999,7 @@ bool Engine::judge(PendingStep& pending, std::string& why)
                 std::ostringstream d;
                 d << "total went " << before << " -> " << after << " (tolerance " << tolerance << ")";
                 v.detail = d.str();
-                violations_.push_back(v);
+                out.push_back(v);
             }
         }
     }
@@ -942,7 +1020,7 @@ bool Engine::judge(PendingStep& pending, std::string& why)
         d << v.count << " cell(s); first " << decl.name << " at (" << first % nx_ << "," << (first / nx_) % ny_ << "," << first / (static_cast<unsigned>(nx_) * ny_)
           << "), declared range [" << decl.lo << ", " << decl.hi << "]";
         v.detail = d.str();
-        violations_.push_back(v);
+        out.push_back(v);
     }
     return true;
 }

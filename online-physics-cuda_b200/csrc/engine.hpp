@@ -55,6 +55,8 @@ struct TermProfile {
     int launches = 0;
     int substeps = 0;
     bool idle = false;
+    bool learned = false;   // the term's learned scheme ran and was kept
+    bool fell_back = false; // it ran, broke a contract, was undone, and the classical scheme ran instead
 };
 
 class Engine {
@@ -85,6 +87,10 @@ public:
 
     void check_every(int steps) { check_every_ = steps < 1 ? 1 : steps; }
     void set_deferred(bool on) { deferred_ = on; }
+    // Learned schemes under guard (Solver::set_learned, Solver.cpp:314-336): a term with learned equations runs them
+    // first on a snapshot of what it writes; a broken contract undoes the step and the classical equations run.
+    void set_learned(bool on) { learned_ = on; }
+    int fallbacks_last_step() const { return fallbacks_; }
 
     const law::Law& law() const { return law_; }
     const ir::Module& module() const { return mod_; }
@@ -132,6 +138,8 @@ private:
     bool run_program(int index, const ir::Program& p, const gen::ProgramPlan& pp, double dt, bool respect, bool check,
         PendingStep& pending, std::string& why);
     bool judge(PendingStep& pending, std::string& why);
+    bool judge_into(const PendingStep& pending, std::vector<Violation>& out, std::string& why);
+    bool apply_term(int t, double dt, bool respect, bool check, PendingStep& pending, std::string& why);
     double scalar_value(int id, bool& ok, std::string& why);
     bool idle(const ir::Program& p) const;
     Bounds bounds_of(int id, const std::vector<Bounds>& fields) const;
@@ -183,6 +191,10 @@ private:
     };
     std::vector<Carry> carry_;
     int own_z0_ = 0, own_z1_ = 0;
+    bool learned_ = false;
+    int fallbacks_ = 0;
+    float* snapshot_ = nullptr;   // what a guarded learned scheme writes, kept to undo it
+    std::size_t snapshot_fields_ = 0;
     bool external_conservation_ = false;
     std::vector<GroupTotals> totals_log_;
     int launches_ = 0;

@@ -78,7 +78,7 @@ class fe_group_totals(ctypes.Structure):
 
 
 class fe_step_info(ctypes.Structure):
-    _fields_ = [("violations", _c.c_int), ("launches", _c.c_int), ("gpu_ms", _c.c_double)]
+    _fields_ = [("violations", _c.c_int), ("launches", _c.c_int), ("gpu_ms", _c.c_double), ("fallbacks", _c.c_int)]
 
 
 class fe_field_info(ctypes.Structure):
@@ -137,6 +137,8 @@ SIGNATURES = {
     "fe_law_field_device_ptr": (_i, [_p, _i, _c.POINTER(_p)]),
     "fe_law_mark_edited": (_i, [_p, _i]),
     "fe_law_set_owned_z": (_i, [_p, _i, _i]),
+    "fe_law_set_learned": (_i, [_p, _i]),
+    "fe_law_term_learned": (_i, [_p, _i]),
     "fe_law_mark_halo": (_i, [_p, _i]),
     "fe_law_set_external_conservation": (_i, [_p, _i]),
     "fe_law_take_totals": (_i, [_p, _c.POINTER(fe_group_totals), _i, _c.POINTER(_i)]),

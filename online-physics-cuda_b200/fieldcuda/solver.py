@@ -152,6 +152,16 @@ class Solver:
     def check_contracts_every(self, steps):
         _lib.check(self._lib.fe_law_check_every(self._h, int(steps)))
 
+    def set_learned(self, on):
+        """Learned schemes under guard (Solver::set_learned): a term's learned equations run first; a step that breaks a
+        contract is undone and taken classically."""
+        _lib.check(self._lib.fe_law_set_learned(self._h, 1 if on else 0))
+
+    def term_learned(self):
+        """Per term in the last step: "learned" (its learned scheme kept), "fell back" (undone), or "classical"."""
+        names = {0: "classical", 1: "learned", 2: "fell back"}
+        return [names.get(self._lib.fe_law_term_learned(self._h, t), "?") for t in range(len(self.term_names))]
+
     def set_deferred(self, on):
         """Judge the contracts at sync() instead of after every checked step."""
         _lib.check(self._lib.fe_law_set_deferred(self._h, 1 if on else 0))
@@ -182,7 +192,7 @@ class Solver:
         return [bool(self._lib.fe_law_term_idle(self._h, t)) for t in range(len(self.term_names))]
 
     def profile(self):
-        return {"launches": self._info.launches, "gpu_ms": self._info.gpu_ms}
+        return {"launches": self._info.launches, "gpu_ms": self._info.gpu_ms, "fallbacks": self._info.fallbacks}
 
     def digest(self):
         """FNV-1a over every field's bits in declaration order (FieldSet::digest)."""
