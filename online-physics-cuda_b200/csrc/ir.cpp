@@ -345,6 +345,37 @@ void json_program(std::ostream& out, const Program& p)
 
 } // namespace
 
+void widen_stages(Module& m)
+{
+    std::vector<int> reads(m.insts.size(), 0);
+    for (const Inst& in : m.insts) {
+        if (in.radius == 0 || in.global || in.net) continue;
+        for (const int a : in.args) reads[static_cast<std::size_t>(a)] += points(in.op);
+    }
+    bool any = false;
+    for (std::size_t id = 0; id < m.insts.size(); ++id) {
+        const Inst& in = m.insts[id];
+        if (m.is_stage(static_cast<int>(id)) || in.shape != Shape::Cell || in.op == Op::Field || reads[id] < 2) continue;
+        if (static_cast<long long>(in.cost) * reads[id] > kInlineBudget) {
+            m.materialized[id] = 1;
+            any = true;
+        }
+    }
+    if (!any) return;
+    for (auto* programs : {&m.terms, &m.learned, &m.derives}) {
+        for (Program& p : *programs) {
+            std::set<int> stages, seen;
+            for (const Equation& eq : p.equations) collect_stages(m, eq.value, stages, seen);
+            p.stages.assign(stages.begin(), stages.end());
+            if (p.max_dt >= 0) {
+                std::set<int> limit, seen_limit;
+                collect_stages(m, p.max_dt, limit, seen_limit);
+                p.limit_stages.assign(limit.begin(), limit.end());
+            }
+        }
+    }
+}
+
 Module lower(const law::Law& law)
 {
     Module m;

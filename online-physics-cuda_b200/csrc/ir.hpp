@@ -72,6 +72,11 @@ struct Module {
 constexpr int kInlineBudget = 48;
 
 Module lower(const law::Law& law);
+// The code generator's own staging on top of the IR's (the IR, and its JSON, stay the reference's): a value that
+// stencil ops read at several offsets, each read inlining its whole expression, is stored once when its inlined cost
+// times the points read passes the inline budget (the IR's rule counts one reader at a time). Stored or inlined it is
+// the same fp32 number, so results do not change. The programs' stage lists are redone; in_place is kept.
+void widen_stages(Module& m);
 std::string to_json(const Module& m, const law::Law& law);
 std::string describe(const Module& m, const law::Law& law);
 

@@ -240,3 +240,26 @@ def test_deferred_judging_keeps_steps_off_the_host(cuda):
     v = s.violations()
     assert [x.step for x in v if x.kind == "conservation"] == [3, 4], v
     s.close()
+
+
+def test_wider_staging_changes_no_bit(cuda):
+    """On a lattice of 2M cells and more the code generator stores values stencils read at several offsets (here the
+    FHN law's third RK4 stage); each z-plane is a sample of its own, so the first planes of such a lattice must match,
+    bit for bit, a small lattice of the same samples planned without it."""
+    from fieldcuda.solver import Solver
+    law = open(os.path.join(ROOT, "tests", "laws", "fhn_rk4.law")).read()
+    rng = np.random.default_rng(8)
+    big_nz, small_nz, n = 128, 8, 128
+    u = rng.normal(size=(big_nz, n, n)).astype(np.float32)
+    v = rng.normal(size=(big_nz, n, n)).astype(np.float32)
+    out = []
+    for nz in (big_nz, small_nz):
+        s = Solver(law, n, n, nz, 2.0 / n)
+        s.set_field("u", u[:nz])
+        s.set_field("v", v[:nz])
+        for _ in range(3):
+            s.step(0.05)
+        out.append((s.values("u")[:small_nz], s.values("v")[:small_nz]))
+        s.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
