@@ -51,18 +51,21 @@ constexpr unsigned kX0 = 0, kH1 = 4 * kGroup, kH2 = 14 * kGroup, kStack = 30 * k
 constexpr unsigned kTZ1 = 0, kTZ2 = 64, kTDH2 = 144, kTDH1 = 224, kTDW1 = 304, kTDW2 = 368, kTDW3 = 432;
 
 // The two layouts. Training keeps the spare groups after H2 (the weight-gradient MMAs read 128 feature rows from X0, H1
-// or H2), dY, dZ2, dZ1 and 512 tensor-memory columns: one CTA an SM. Inference needs X0 | H1 | H2 and the weights
-// (65 KB) and 128 columns (Y reuses Z1's, consumed by then): three CTAs an SM.
+// or H2), dY, dZ2, dZ1 and 512 tensor-memory columns: one CTA an SM. Inference needs X0 | H1 and the weights (45 KB;
+// H2 is written over H1 once the MMA that read H1 has completed) and 128 columns (Y reuses Z1's, consumed by then):
+// four CTAs an SM, the tensor memory's 512 columns (the size is padded so a fifth never waits for columns).
 template <bool TRAIN>
 struct Layout {
-    static constexpr unsigned WB1 = TRAIN ? kStack : 24 * kGroup;
+    static constexpr unsigned H2 = TRAIN ? kH2 : kH1;
+    static constexpr unsigned WB1 = TRAIN ? kStack : 14 * kGroup;
     static constexpr unsigned WB2 = WB1 + kW1 * 2, WB3 = WB2 + kW2 * 2, WEnd = WB3 + kW3 * 2;
     static constexpr unsigned DY = WEnd, DZ2 = DY + 2 * kGroup, DZ1 = DZ2 + 8 * kGroup;
     static constexpr unsigned BAR = TRAIN ? DZ1 + 8 * kGroup : WEnd;
-    static constexpr unsigned SMEM = BAR + 64;
+    static constexpr unsigned SMEM = TRAIN ? BAR + 64 : 46592u;
     static constexpr unsigned TY = TRAIN ? 128u : 0u;
     static constexpr unsigned TCOLS = TRAIN ? 512u : 128u;
-    static constexpr int PER_SM = TRAIN ? 1 : 3;
+    static constexpr int PER_SM = TRAIN ? 1 : 4;
+    static_assert(TRAIN || (BAR + 64 <= SMEM && 5 * SMEM > 232448u), "inference: four CTAs an SM, never five");
 };
 constexpr unsigned kWaitLimit = 1u << 22;
 
@@ -291,12 +294,12 @@ __global__ void __launch_bounds__(kThreadsC, Layout<TRAIN>::PER_SM) corr_kernel(
         }
         if (!(ok = mma_wait(bar, phase, a.err))) break;
         // 3. H2 = ReLU(Z2); Y = H2 W3.
-        hidden_out(lane_base + kTZ2, sm, kH2, t);
+        hidden_out(lane_base + kTZ2, sm, L::H2, t);
         hand_over();
         if (t == 0) {
             tc_after();
             for (int k = 0; k < 5; ++k) {
-                mma(tbase + L::TY, sdesc(s0 + kH2 + k * 2 * kGroup, kGroup, 128), sdesc(s0 + L::WB3 + k * 2 * 128, 128, (80 / 8) * 128),
+                mma(tbase + L::TY, sdesc(s0 + L::H2 + k * 2 * kGroup, kGroup, 128), sdesc(s0 + L::WB3 + k * 2 * 128, 128, (80 / 8) * 128),
                     idesc(128, 16, false, true), k > 0);
             }
             mma_commit(bar);
