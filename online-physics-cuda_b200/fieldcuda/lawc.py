@@ -11,8 +11,9 @@ the scripts that drive it (the bench drivers, tools/lawjax) run unchanged with t
 
 Scenes are the reference's text format (src/field/Scene.hpp:9-17): grid, law, fill, box, ball, noise, param; dumps
 are raw float32 per field plus meta.json (Scene.cpp:112-135). The solves run on the GPU; the reference's CPU solver is
-not part of this backend, so --backend cpu and --compare are refused, and so are --vjp and --learned (see
-fieldcuda.adjoint for reverse mode).
+not part of this backend, so --backend cpu and --compare are refused, and so is --vjp (fieldcuda.adjoint is reverse
+mode). --learned runs the terms' learned schemes under guard (main.cpp:260): a learned step that breaks a contract is
+undone and taken classically, and the undone steps are counted in --profile and --json as the reference counts them.
 """
 import argparse
 import json
@@ -133,6 +134,20 @@ def load_fields(solver, directory):
         solver.set_field(n, v.reshape(solver.shape))
 
 
+def print_profile(solver, step_ms):
+    """One step's profile in the reference's layout (main.cpp:71-92): the card's time and launches, the undone learned
+    steps, then per running term its substeps and whether its learned scheme was kept or fell back."""
+    p = solver.profile()
+    line = f"  B200: step {step_ms:.3f} ms (card {p['gpu_ms']:.3f} ms, {p['launches']} launches)"
+    if p["fallbacks"] > 0:
+        line += f", {p['fallbacks']} learned step(s) undone"
+    print(line)
+    marks = {"learned": "  learned", "fell back": "  FELL BACK"}
+    for name, idle, sub, how in zip(solver.term_names, solver.idle_terms(), solver.last_substeps(), solver.term_learned()):
+        if not idle:
+            print(f"    {name:<22} x{sub}{marks.get(how, '')}")
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="lawc", description="the law compiler and runner on the B200 backend")
     ap.add_argument("laws", nargs="*")
@@ -164,7 +179,7 @@ def main(argv=None):
         print(f"no {args.backend} backend here: this lawc runs the B200 backend only", file=sys.stderr)
         return 1
     for flag, what in ((args.compare, "--compare (the reference's CPU solver is not part of this backend)"),
-                       (args.vjp, "--vjp (reverse mode is fieldcuda.adjoint)"), (args.learned, "--learned (no nets on this backend)")):
+                       (args.vjp, "--vjp (reverse mode is fieldcuda.adjoint)")):
         if flag:
             print(f"not in this lawc: {what}", file=sys.stderr)
             return 2
@@ -190,6 +205,15 @@ def main(argv=None):
 
     from . import _lib
     from .solver import Solver, cuda_source, ir_json, ir_listing
+    try:
+        nets = json.loads(ir_json(text))["nets"]
+    except _lib.FeError as e:
+        print(e, file=sys.stderr)
+        return 1
+    for net in nets:
+        if not net["loaded"]:
+            print(f"note: net '{net['name']}' has no weights at {net['file']} (it starts untrained: its output is 0)",
+                  file=sys.stderr)
     try:
         if args.ir:
             print(ir_listing(text), end="")
@@ -220,6 +244,8 @@ def main(argv=None):
         print(e, file=sys.stderr)
         return 1
     try:
+        if args.learned:
+            s.set_learned(True)
         for name, value in scene.params + [(n, float(v)) for n, v in args.param]:
             if not s.set_param(name, value):
                 print(f"the law has no param '{name}'", file=sys.stderr)
@@ -234,18 +260,19 @@ def main(argv=None):
     except ValueError as e:
         print(e, file=sys.stderr)
         return 1
-    print(f"{len(s.field_names)} fields, {len(s.term_names)} terms, 0 nets; grid {nx}x{ny}x{nz} at {h:g} m; {args.steps} steps of "
+    print(f"{len(s.field_names)} fields, {len(s.term_names)} terms, {len(nets)} nets; grid {nx}x{ny}x{nz} at {h:g} m; {args.steps} steps of "
           f"{args.dt:g} s on B200")
     if args.dump:
         dump_fields(s, os.path.join(args.dump, "step_0"), args.dump_only)
     total = 0.0
     timed, gpu = [], 0.0
-    violations = 0
+    violations = fallbacks = 0
     for step in range(1, args.steps + 1):
         t0 = time.perf_counter()
         s.step(args.dt)
         ms = (time.perf_counter() - t0) * 1e3
         total += ms
+        fallbacks += s.profile()["fallbacks"]
         if step > args.warmup:
             timed.append(ms)
             gpu += s.profile()["gpu_ms"]
@@ -257,8 +284,7 @@ def main(argv=None):
         if args.dump and args.every > 0 and step % args.every == 0:
             dump_fields(s, os.path.join(args.dump, f"step_{step}"), args.dump_only)
         if args.profile and (step == 1 or step == args.steps):
-            p = s.profile()
-            print(f"  step {step}: {p['launches']} launches, {p['gpu_ms']:.3f} ms on the card")
+            print_profile(s, ms)
     if args.dump and (args.every <= 0 or args.steps % args.every != 0):
         dump_fields(s, os.path.join(args.dump, f"step_{args.steps}"), args.dump_only)
     print(f"mean step {total / args.steps:g} ms, {violations} contract violation(s)")
@@ -266,7 +292,7 @@ def main(argv=None):
         out = {"backend": "B200", "cells": nx * ny * nz, "steps": len(timed),
                "mean_ms": (sum(timed) / len(timed)) if timed else 0.0,
                "median_ms": sorted(timed)[len(timed) // 2] if timed else 0.0,
-               "gpu_ms": gpu / len(timed) if timed else 0.0, "violations": violations, "fallbacks": 0,
+               "gpu_ms": gpu / len(timed) if timed else 0.0, "violations": violations, "fallbacks": fallbacks,
                "substeps": s.last_substeps(), "terms": {t: 0.0 for t in s.term_names}}
         with open(args.json, "w") as f:
             f.write(json.dumps(out) + "\n")

@@ -30,3 +30,19 @@ def test_scene_run_matches_the_reference_lawc(cuda, tmp_path, monkeypatch):
         got = np.fromfile(dump / f"step_{meta['steps']}" / f"{name}.bin", np.float32).reshape(9, 14, 20).astype(np.float64)
         want = z[f"step{meta['steps']}_{name}"].astype(np.float64)
         assert np.abs(got - want).max() <= 1e-4 * max(np.abs(want).max(), 1e-6), name
+
+
+def test_learned_run_counts_the_undone_steps(cuda, tmp_path, monkeypatch, capsys):
+    from fieldcuda import lawc
+    monkeypatch.chdir(ROOT)
+    js = tmp_path / "g.json"
+    rc = lawc.main(["--scene", "tests/scenes/guarded.scene", "--steps", "30", "--dt", "0.3", "--learned", "--profile",
+                    "--json", str(js)])
+    assert rc == 0
+    out = json.loads(js.read_text())
+    printed = capsys.readouterr().out
+    assert "1 fields, 1 terms, 1 nets" in printed
+    assert out["violations"] == 0 and 0 < out["fallbacks"] <= 30
+    assert "learned step(s) undone" in printed
+    rc = lawc.main(["--scene", "tests/scenes/guarded.scene", "--steps", "5", "--dt", "0.3", "--json", str(js)])
+    assert rc == 0 and json.loads(js.read_text())["fallbacks"] == 0
