@@ -7,6 +7,8 @@
 #include <map>
 #include <set>
 #include <cstdlib>
+#include <cstdint>
+#include <cstring>
 #include <sstream>
 
 namespace fe::gen {
@@ -534,6 +536,7 @@ private:
             plan_.net_blob.insert(plan_.net_blob.end(), net.in_scale.begin(), net.in_scale.end());
             const std::size_t os = plan_.net_blob.size();
             plan_.net_blob.push_back(net.out_scale);
+            net_at_.push_back(NetAt{w0, sh, sc, os, pack_half(net)});
             const std::string act = net.act == "tanh" ? "tanhf(v)" : net.act == "relu" ? "(v > 0.f ? v : 0.f)" : net.act == "silu" ? "v / (1.f + expf(-v))" : "v";
             f << "__device__ __forceinline__ float fe_act" << k << "(float v) { return " << act << "; }\n";
             f << "__device__ __forceinline__ void fe_net" << k << "(const float* in, float* out) {\n";
@@ -553,6 +556,7 @@ private:
             f << "#pragma unroll\n    for (int o = 0; o < " << net.sizes.back() << "; ++o) out[o] = h" << net.layers() << "[o] * FE_NET[" << os << "];\n}\n";
         }
         out_ << "__device__ float FE_NET[" << std::max<std::size_t>(1, plan_.net_blob.size()) << "];\n";
+        out_ << "__device__ __align__(16) unsigned short FE_NETB[" << std::max<std::size_t>(8, plan_.net_bf16.size()) << "];\n";
         out_ << R"(// The flux limiter of flux(): the same on both sides of a face, so the flux stays antisymmetric; within one step of dt
 // no cell goes below the moved field's least or above its most (Law.cpp:672-689).
 __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, double lo, double hi, float dt)
@@ -928,6 +932,222 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
         return true;
     }
 
+    static int pad16(int v) { return (v + 15) / 16 * 16; }
+
+    // BF16, round to nearest even (NaN kept a NaN).
+    static unsigned short to_bf16(float v)
+    {
+        std::uint32_t u = 0;
+        std::memcpy(&u, &v, sizeof(u));
+        if ((u & 0x7F800000u) == 0x7F800000u && (u & 0x007FFFFFu) != 0u) return static_cast<unsigned short>((u >> 16) | 0x40u);
+        u += 0x7FFFu + ((u >> 16) & 1u);
+        return static_cast<unsigned short>(u >> 16);
+    }
+
+    // A `half` net's weights into FE_NETB: per layer the K x N matrix (K = inputs, N = outputs, each padded to 16 with
+    // zeros) in BF16, in the no-swizzle core-matrix layout with K rows, element (k, n) = W[n][k]; returns the net's byte
+    // offset (every layer starts on a 512-byte boundary). A net without `half` packs nothing.
+    std::size_t pack_half(const law::NetDecl& net)
+    {
+        const std::size_t start = plan_.net_bf16.size() * 2;
+        if (!net.half) return start;
+        for (int l = 0; l < net.layers(); ++l) {
+            const int ni = net.sizes[static_cast<std::size_t>(l)];
+            const int no = net.sizes[static_cast<std::size_t>(l) + 1];
+            const int K = pad16(ni), N = pad16(no);
+            const std::size_t base = plan_.net_bf16.size();
+            plan_.net_bf16.resize(base + static_cast<std::size_t>(K) * N, 0);
+            const std::size_t off = net.weight_offset(l);
+            for (int k = 0; k < ni; ++k) {
+                for (int n = 0; n < no; ++n) {
+                    const unsigned byte = static_cast<unsigned>(((n >> 3) * (K >> 3) + (k >> 3)) * 128 + (k & 7) * 16 + (n & 7) * 2);
+                    plan_.net_bf16[base + byte / 2] = to_bf16(net.weights[off + static_cast<std::size_t>(n) * ni + static_cast<std::size_t>(k)]);
+                }
+            }
+        }
+        return start;
+    }
+
+    // A net op whose net is declared `half` (the reference's tensor-core nets): one stage kernel on tcgen05
+    // (fe_device.cuh's fe_net_pass) that stores the op's value at every cell in the stage's slot. The P traits give the
+    // net's padded shapes, its parameters' places, the inputs of each of a cell's evaluations (mlp: its arguments at
+    // the cell; flux: the moved field and its companions on both sides of each of the six faces, both ways round;
+    // ldiffuse: each face's normalised window of four cells and k's face value times dt / h^2, both ways round) and the
+    // op's own FP32 arithmetic around the net (Law.cpp:1298-1438; CudaCodegen.cpp:718-840).
+    bool emit_net(const std::string& tag, int id, Launch& L, std::string& why)
+    {
+        const Inst& in = at(id);
+        const law::NetDecl& net = law_.nets[static_cast<std::size_t>(in.index)];
+        const NetAt& na = net_at_[static_cast<std::size_t>(in.index)];
+        const int layers = net.layers();
+        std::vector<int> kp, np, no, wb, bias;
+        int wbytes = 0, nmax = 16, kmax = 16;
+        for (int l = 0; l < layers; ++l) {
+            const int ni = net.sizes[static_cast<std::size_t>(l)];
+            const int o = net.sizes[static_cast<std::size_t>(l) + 1];
+            if (o > 256 || ni > 256) {
+                why = "net '" + net.name + "' is declared half, and the tensor-core form takes layers at most 256 wide";
+                return false;
+            }
+            kp.push_back(pad16(ni));
+            np.push_back(pad16(o));
+            no.push_back(o);
+            wb.push_back(wbytes);
+            bias.push_back(static_cast<int>(na.w0 + net.weight_offset(l) + static_cast<std::size_t>(ni) * o));
+            wbytes += pad16(ni) * pad16(o) * 2;
+            nmax = std::max(nmax, pad16(o));
+            kmax = std::max(kmax, pad16(ni));
+        }
+        int e = 1, nin = static_cast<int>(in.args.size());
+        if (in.op == Op::Flux) {
+            e = 12;
+            nin = 2 * (static_cast<int>(in.args.size()) - 2);
+        } else if (in.op == Op::LDiffuse) {
+            e = 12;
+            nin = 5;
+        }
+        const int nout = net.sizes.back();
+        if (nin != net.sizes.front() || (in.op == Op::LDiffuse && nout != 4)) {
+            why = "net '" + net.name + "' does not fit its op";
+            return false;
+        }
+        const int ec = std::max(1, std::min(e, 128 / nmax));
+        int tcols = 32;
+        while (tcols < ec * nmax) tcols *= 2;
+        const int per_sm = std::min(8, 512 / tcols);
+        const unsigned a_bytes = static_cast<unsigned>(128 * kmax * 2);
+        const unsigned need = static_cast<unsigned>(ec) * a_bytes + static_cast<unsigned>(wbytes) + 16;
+        // Enough shared memory that no more than per_sm CTAs fit on an SM (228 KB, 1 KB reserved a CTA): each holds
+        // tcols tensor-memory columns, and an SM has 512.
+        const unsigned cap = static_cast<unsigned>(233472 / (per_sm + 1) - 1024 + 128) / 128 * 128;
+        const unsigned smem = std::max(need, cap);
+        if (smem > 227u * 1024u) {
+            why = "net '" + net.name + "' is declared half, and its tensor-core tiles need more shared memory than a CTA has";
+            return false;
+        }
+
+        PassBuild pb;
+        const Radius r = axis_radius(in);
+        for (const int arg : in.args) walk(pb, arg, r, false);
+        std::ostringstream f;
+        const std::string ns = "fe_" + tag;
+        f << "namespace " << ns << " {\n";
+        std::vector<int> roots(in.args.begin(), in.args.end());
+        emit_functions(f, pb, roots, false);
+        auto arg = [&](std::size_t k, const std::string& x, const std::string& y, const std::string& z) {
+            return "v" + std::to_string(in.args[k]) + "<false>(c, " + x + ", " + y + ", " + z + ")";
+        };
+        auto fn = [&](const char* type, const char* name, const std::vector<int>& v) {
+            f << "    static __device__ __forceinline__ constexpr " << type << " " << name << "(int l) { ";
+            for (std::size_t k = 0; k < v.size(); ++k) f << "if (l == " << k << ") return " << v[k] << "; ";
+            f << "return 0; }\n";
+        };
+        // The face f (0..5: -x, +x, -y, +y, -z, +z) of a cell: its lower cell i and upper cell j (clamped: a face past
+        // the lattice's edge is never used), and whether it is open.
+        f << "__device__ __forceinline__ void face_cells(int f, int x, int y, int z, int& ix, int& iy, int& iz, int& jx, int& jy, int& jz) {\n"
+          << "    const int ax = f >> 1; ix = x; iy = y; iz = z;\n"
+          << "    if ((f & 1) == 0) { ix = fe_ex(x - (ax == 0)); iy = fe_ey(y - (ax == 1)); iz = fe_ez(z - (ax == 2)); }\n"
+          << "    jx = fe_ex(ix + (ax == 0)); jy = fe_ey(iy + (ax == 1)); jz = fe_ez(iz + (ax == 2)); }\n"
+          << "__device__ __forceinline__ bool face_open(int f, int x, int y, int z) {\n"
+          << "    const int ax = f >> 1; const int q = ax == 0 ? x : (ax == 1 ? y : z); const int n = ax == 0 ? NX : (ax == 1 ? NY : NZ);\n"
+          << "    return (f & 1) ? q + 1 < n : q > 0; }\n";
+        if (in.op == Op::LDiffuse) {
+            // The window F[i-1] F[i] | F[j] F[j+1] of the face between i = (x, y, z) and its +AX neighbour j (edge
+            // cells repeat), and k's face value (the harmonic mean, in double): the fp32 form's arithmetic.
+            f << "template <int AX, class C> __device__ __forceinline__ void window(const C& c, int x, int y, int z, float* w, float& kf) {\n"
+              << "    const int jx = fe_ex(x + (AX == 0)), jy = fe_ey(y + (AX == 1)), jz = fe_ez(z + (AX == 2));\n"
+              << "    const int q = AX == 0 ? x : (AX == 1 ? y : z); const int count = AX == 0 ? NX : (AX == 1 ? NY : NZ);\n"
+              << "    const int mx = q > 0 ? x - (AX == 0) : x, my = q > 0 ? y - (AX == 1) : y, mz = q > 0 ? z - (AX == 2) : z;\n"
+              << "    const int px = q + 2 < count ? jx + (AX == 0) : jx, py = q + 2 < count ? jy + (AX == 1) : jy, pz = q + 2 < count ? jz + (AX == 2) : jz;\n"
+              << "    w[0] = " << arg(1, "mx", "my", "mz") << "; w[1] = " << arg(1, "x", "y", "z") << "; w[2] = " << arg(1, "jx", "jy", "jz")
+              << "; w[3] = " << arg(1, "px", "py", "pz") << ";\n"
+              << "    const double ka = " << arg(0, "x", "y", "z") << ", kb = " << arg(0, "jx", "jy", "jz") << ";\n"
+              << "    kf = static_cast<float>((ka + kb) > 0.0 ? 2.0 * ka * kb / (ka + kb) : 0.0); }\n"
+              << "template <class C> __device__ __forceinline__ void face_window(const C& c, int f, int x, int y, int z, float* w, float& kf) {\n"
+              << "    int ix, iy, iz, jx, jy, jz; face_cells(f, x, y, z, ix, iy, iz, jx, jy, jz);\n"
+              << "    const int ax = f >> 1;\n"
+              << "    if (ax == 0) window<0>(c, ix, iy, iz, w, kf); else if (ax == 1) window<1>(c, ix, iy, iz, w, kf); else window<2>(c, ix, iy, iz, w, kf); }\n"
+              << "__device__ __forceinline__ float after_net(const float* yw, const float* w, float kf) {\n"
+              << "    const float mean = 0.25f * (yw[0] + yw[1] + yw[2] + yw[3]);\n"
+              << "    const float base[4] = {0.f, -1.f, 1.f, 0.f}; float acc = 0.f;\n"
+              << "#pragma unroll\n    for (int q = 0; q < 4; ++q) acc += (base[q] + (yw[q] - mean)) * w[q];\n"
+              << "    return -kf / FE_H * acc; }\n";
+        }
+        f << "struct P {\n"
+          << "    static constexpr int NX = ::NX, NY = ::NY, NZ = ::NZ;\n"
+          << "    static constexpr int E = " << e << ", EC = " << ec << ", NIN = " << nin << ", NOUT = " << nout << ", L = " << layers
+          << ", NMAX = " << nmax << ", KP0 = " << kp[0] << ";\n"
+          << "    static constexpr unsigned TCOLS = " << tcols << "u, A_BYTES = " << a_bytes << "u, W_BYTES = " << wbytes << "u, WOFF = " << na.bf16_bytes
+          << "u;\n"
+          << "    static constexpr int SHIFT = " << na.shift << ", SCALE = " << na.scale << ", OSCALE = " << na.oscale << ";\n";
+        fn("int", "kp", kp);
+        fn("int", "np", np);
+        fn("int", "no", no);
+        fn("unsigned", "wb", wb);
+        fn("int", "bias", bias);
+        f << "    static __device__ __forceinline__ float act(float v) { return fe_act" << in.index << "(v); }\n";
+        f << "    template <class C> static __device__ __forceinline__ void input(const C& c, int x, int y, int z, int e, float* xin) {\n";
+        if (in.op == Op::Mlp) {
+            for (std::size_t k = 0; k < in.args.size(); ++k) f << "        xin[" << k << "] = " << arg(k, "x", "y", "z") << ";\n";
+            f << "    }\n"
+              << "    template <class C> static __device__ __forceinline__ float finish(const C&, int, int, int, const float (*yv)[NOUT]) { return yv[0][0]; }\n";
+        } else if (in.op == Op::Flux) {
+            const std::size_t m = in.args.size() - 2;
+            char bounds[96];
+            std::snprintf(bounds, sizeof(bounds), "%.17g, %.17g", at(in.args[m]).number, at(in.args[m + 1]).number);
+            f << "        int ix, iy, iz, jx, jy, jz; face_cells(e >> 1, x, y, z, ix, iy, iz, jx, jy, jz);\n"
+              << "        if (e & 1) { int t = ix; ix = jx; jx = t; t = iy; iy = jy; jy = t; t = iz; iz = jz; jz = t; }\n";
+            for (std::size_t k = 0; k < m; ++k) {
+                f << "        xin[" << k << "] = " << arg(k, "ix", "iy", "iz") << "; xin[" << m + k << "] = " << arg(k, "jx", "jy", "jz") << ";\n";
+            }
+            f << "    }\n"
+              << "    template <class C> static __device__ __forceinline__ float finish(const C& c, int x, int y, int z, const float (*yv)[NOUT]) {\n"
+              << "        float o = 0.f;\n"
+              << "#pragma unroll\n        for (int f = 0; f < 6; ++f) {\n"
+              << "            if (!face_open(f, x, y, z)) continue;\n"
+              << "            int ix, iy, iz, jx, jy, jz; face_cells(f, x, y, z, ix, iy, iz, jx, jy, jz);\n"
+              << "            const float g = fe_limit_face(0.5f * (yv[2 * f][0] - yv[2 * f + 1][0]), " << arg(0, "ix", "iy", "iz") << ", "
+              << arg(0, "jx", "jy", "jz") << ", " << bounds << ", c.dt);\n"
+              << "            if (f & 1) o -= g; else o += g;\n"
+              << "        }\n"
+              << "        return o / FE_H; }\n";
+        } else {
+            f << "        float w[4], kf; face_window(c, e >> 1, x, y, z, w, kf);\n"
+              << "        if (e & 1) { float t = w[0]; w[0] = w[3]; w[3] = t; t = w[1]; w[1] = w[2]; w[2] = t; }\n"
+              << "        const float centre = 0.5f * (w[1] + w[2]); float spread = 1e-6f;\n"
+              << "#pragma unroll\n        for (int q = 0; q < 4; ++q) spread = fmaxf(spread, fabsf(w[q] - centre));\n"
+              << "#pragma unroll\n        for (int q = 0; q < 4; ++q) xin[q] = (w[q] - centre) / spread;\n"
+              << "        xin[4] = kf * c.dt / (FE_H * FE_H);\n"
+              << "    }\n"
+              << "    template <class C> static __device__ __forceinline__ float finish(const C& c, int x, int y, int z, const float (*yv)[NOUT]) {\n"
+              << "        float o = 0.f;\n"
+              << "#pragma unroll\n        for (int f = 0; f < 6; ++f) {\n"
+              << "            if (!face_open(f, x, y, z)) continue;\n"
+              << "            float w[4], kf; face_window(c, f, x, y, z, w, kf);\n"
+              << "            const float mirror[4] = {w[3], w[2], w[1], w[0]};\n"
+              << "            const float g = 0.5f * (after_net(yv[2 * f], w, kf) - after_net(yv[2 * f + 1], mirror, kf));\n"
+              << "            if (f & 1) o -= g; else o += g;\n"
+              << "        }\n"
+              << "        return o / FE_H; }\n";
+        }
+        f << "};\n}\n";
+        L.kind = Launch::Net;
+        L.sources = pb.sources;
+        L.slab = false;
+        int rz = 0;
+        for (const Radius& q : pb.reach) rz = std::max(rz, q.z);
+        L.rz = rz;
+        L.outs = {Buf{Buf::Slot, plan_.slot_of[static_cast<std::size_t>(id)]}};
+        L.checked_fields = {-1};
+        L.smem = smem;
+        L.per_sm = per_sm;
+        L.kernel = "fe_net_" + tag;
+        f << "extern \"C\" __global__ void __launch_bounds__(128) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_net_pass<" << ns
+          << "::P>(a, FE_NETB, FE_NET); }\n";
+        out_ << f.str();
+        return true;
+    }
+
     // Stages in order; consecutive stored stages that do not read one another share a pass.
     bool emit_stages(const std::string& tag, const std::vector<int>& stages, std::vector<Launch>& launches, std::string& why)
     {
@@ -951,6 +1171,13 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
         };
         for (const int s : stages) {
             const Inst& in = at(s);
+            if (in.net && law_.nets[static_cast<std::size_t>(in.index)].half) {
+                if (!flush()) return false;
+                Launch L;
+                if (!emit_net(tag + "n" + std::to_string(n++), s, L, why)) return false;
+                launches.push_back(L);
+                continue;
+            }
             if (in.op == Op::Tridiag || in.global) {
                 if (!flush()) return false;
                 Launch L;
@@ -1038,6 +1265,12 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
     double h_;
     Plan& plan_;
     std::map<int, int> flag_of_; // distance / poisson inst -> its change flag
+    // Per net: where its parameters sit in FE_NET (weights, input shift, input scale, output scale) and, for a `half`
+    // net, its BF16 weights' byte offset in FE_NETB.
+    struct NetAt {
+        std::size_t w0, shift, scale, oscale, bf16_bytes;
+    };
+    std::vector<NetAt> net_at_;
     std::ostringstream out_;
 };
 

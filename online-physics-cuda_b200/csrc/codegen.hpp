@@ -27,7 +27,7 @@ struct Source {
 };
 
 struct Launch {
-    enum Kind : unsigned char { Pass, TridiagX, TridiagYZ, Reduce, Distance, Poisson } kind = Pass;
+    enum Kind : unsigned char { Pass, TridiagX, TridiagYZ, Reduce, Distance, Poisson, Net } kind = Pass;
     std::string kernel;       // the slab (TMA) kernel, or the only one
     std::string plain_kernel; // the plain-load twin of a Pass
     std::vector<Source> sources;
@@ -45,6 +45,9 @@ struct Launch {
     int aux = -1;
     int flag = -1;
     int iterations = 0;
+    // Net: a `half` net op on the tensor cores (128 threads a CTA, persistent); at most this many CTAs an SM hold
+    // tensor memory at once (the shared memory asked for keeps more from being resident).
+    int per_sm = 0;
 };
 
 struct ProgramPlan {
@@ -65,6 +68,7 @@ struct Plan {
     int flags = 0;                // change flags of the distance and poisson ops
     std::vector<std::pair<int, unsigned>> slot_fill; // slots to fill at creation with a bit pattern
     std::vector<float> net_blob;  // the nets' parameters as the module's FE_NET holds them (weights, shift, scale, out scale)
+    std::vector<unsigned short> net_bf16; // the `half` nets' weights as FE_NETB holds them (BF16, per layer K x N, core layout)
     std::vector<char> pingpong;   // per field: has a next buffer
     std::vector<ProgramPlan> terms, learned, derives;
     std::string source;           // the translation unit

@@ -103,6 +103,20 @@ bool Engine::create(const std::vector<law::Source>& sources, int nx, int ny, int
             return false;
         }
     }
+    if (!plan_.net_bf16.empty()) {
+        // The `half` nets' BF16 weights, in the layout their tensor-core stage kernels copy into shared memory.
+        CUdeviceptr netb = 0;
+        if (!cu_ok(d.moduleGetGlobal(&netb, &bytes, module_, "FE_NETB"), "FE_NETB", why)) return false;
+        if (bytes < plan_.net_bf16.size() * sizeof(unsigned short)) {
+            why = "internal: FE_NETB is smaller than the half nets' weights";
+            return false;
+        }
+        if (!cuda_ok(cudaMemcpy(reinterpret_cast<void*>(netb), plan_.net_bf16.data(), plan_.net_bf16.size() * sizeof(unsigned short),
+                         cudaMemcpyHostToDevice),
+                "half nets", why)) {
+            return false;
+        }
+    }
     if (!cuda_ok(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate", why)) return false;
     if (!cuda_ok(cudaEventCreate(&ev0_), "cudaEventCreate", why) || !cuda_ok(cudaEventCreate(&ev1_), "cudaEventCreate", why)) return false;
 
@@ -356,6 +370,14 @@ bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* r
         block = 256;
         gx = static_cast<unsigned>(std::min<std::size_t>((cells_ + 255) / 256, static_cast<std::size_t>(sms_) * 4));
         break;
+    case gen::Launch::Net: {
+        // Persistent: one CTA of 128 threads a 128-cell tile, as many CTAs as can hold tensor memory at once.
+        const std::size_t tiles = (cells_ + 127) / 128;
+        block = 128;
+        gx = static_cast<unsigned>(std::min<std::size_t>(tiles, static_cast<std::size_t>(sms_) * static_cast<std::size_t>(L.per_sm)));
+        smem = L.smem;
+        break;
+    }
     case gen::Launch::Distance:
     case gen::Launch::Poisson:
         break; // launch_solve, above
@@ -365,7 +387,7 @@ bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* r
         std::any_of(L.checked_fields.begin(), L.checked_fields.end(), [](int f) { return f >= 0; })) {
         name += "_halo";
     }
-    if (static_cast<std::size_t>(a.blocks) * 4 * FE_MAX_OUT > partial_doubles_) {
+    if (L.kind != gen::Launch::Net && static_cast<std::size_t>(a.blocks) * 4 * FE_MAX_OUT > partial_doubles_) {
         why = "internal: too few partial sums for a launch";
         return false;
     }
@@ -458,7 +480,7 @@ void plan_z_reach(const gen::Plan& plan, int& reach, bool& reductions, bool& z_s
     reductions = false;
     z_solves = false;
     auto count = [&](const gen::Launch& L) {
-        if (L.kind == gen::Launch::Pass) reach += L.rz;
+        if (L.kind == gen::Launch::Pass || L.kind == gen::Launch::Net) reach += L.rz;
         if (L.kind == gen::Launch::Reduce || L.kind == gen::Launch::Distance || L.kind == gen::Launch::Poisson) reductions = true;
         if (L.kind == gen::Launch::TridiagYZ && L.axis == 2) z_solves = true;
     };

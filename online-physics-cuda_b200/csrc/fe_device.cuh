@@ -977,6 +977,205 @@ __device__ __forceinline__ void fe_tridiag_yz_pass(const FePassArgs& a)
     }
 }
 
+// ---- tcgen05 (the fifth-generation tensor cores), for the law's `half` nets ----------------------------------------
+// Operands are BF16 matrices in shared memory in the canonical no-swizzle core-matrix layout: a core matrix is 8 rows
+// of 16 bytes, element (r, c) of an R-row matrix at ((c / 8) (R / 8) + r / 8) 128 + (r % 8) 16 + (c % 8) 2 bytes.
+// Accumulators are FP32 in tensor memory, one lane a row. One thread issues the MMAs and commits them to an mbarrier
+// that every thread waits on with a bounded wait.
+__device__ __forceinline__ unsigned fe_tc_core(int r, int c, int R)
+{
+    return static_cast<unsigned>(((c >> 3) * (R >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (c & 7) * 2);
+}
+
+// Shared-memory matrix descriptor: start, leading and stride byte offsets (16-byte units), sm_100 version 1, no swizzle.
+__device__ __forceinline__ fe_u64 fe_tc_sdesc(unsigned saddr, unsigned lbo, unsigned sbo)
+{
+    fe_u64 d = static_cast<fe_u64>((saddr >> 4) & 0x3FFFu);
+    d |= static_cast<fe_u64>((lbo >> 4) & 0x3FFFu) << 16;
+    d |= static_cast<fe_u64>((sbo >> 4) & 0x3FFFu) << 32;
+    d |= 1ull << 46;
+    return d;
+}
+
+// kind::f16 instruction descriptor: FP32 accumulator, BF16 A (K-major) and B (MN-major), M x N.
+__device__ __forceinline__ unsigned fe_tc_idesc(int M, int N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | (static_cast<unsigned>(N >> 3) << 17) | (static_cast<unsigned>(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void fe_tc_mma(unsigned dtmem, fe_u64 a, fe_u64 b, unsigned id, unsigned accumulate)
+{
+    asm volatile("{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                 ::"r"(dtmem), "l"(a), "l"(b), "r"(id), "r"(accumulate)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fe_tc_commit(fe_u64* bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(fe_smem(bar)) : "memory");
+}
+
+__device__ __forceinline__ void fe_tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fe_tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fe_tc_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// 16 consecutive FP32 columns of this thread's tensor-memory lane.
+__device__ __forceinline__ void fe_tc_ld16(unsigned taddr, float* r)
+{
+    unsigned x[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                 : "=r"(x[0]), "=r"(x[1]), "=r"(x[2]), "=r"(x[3]), "=r"(x[4]), "=r"(x[5]), "=r"(x[6]), "=r"(x[7]), "=r"(x[8]),
+                   "=r"(x[9]), "=r"(x[10]), "=r"(x[11]), "=r"(x[12]), "=r"(x[13]), "=r"(x[14]), "=r"(x[15])
+                 : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) r[i] = __uint_as_float(x[i]);
+}
+
+// Two floats as BF16 (round to nearest even), the first in the low half.
+__device__ __forceinline__ unsigned fe_tc_bf16x2(float lo, float hi)
+{
+    unsigned r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
+// Row r's columns c0 .. c0 + 7 of a 128-row operand tile, one 16-byte store.
+__device__ __forceinline__ void fe_tc_put8(unsigned char* tile, int r, int c0, const float* v)
+{
+    const uint4 q = make_uint4(fe_tc_bf16x2(v[0], v[1]), fe_tc_bf16x2(v[2], v[3]), fe_tc_bf16x2(v[4], v[5]), fe_tc_bf16x2(v[6], v[7]));
+    *reinterpret_cast<uint4*>(tile + fe_tc_core(r, c0, 128)) = q;
+}
+
+// A net op whose net is declared `half` (the reference's tensor-core nets, CudaNet.cpp:175-277), as one stage kernel:
+// 128 threads, thread t owns cell t of a 128-cell tile and row / tensor-memory lane t, persistent over tiles. A cell
+// needs P::E evaluations of the net (mlp 1; flux and ldiffuse 12: six faces, both ways round); P::EC of them at a time
+// are 128-row tiles in shared memory, and each layer is P::EC M = 128 MMAs (K = 16 a step) into their own accumulator
+// columns. Between layers every thread reads its row back, adds the FP32 bias, applies the activation and writes the
+// next layer's BF16 operand over the last one (whose MMAs have completed). The op's own arithmetic around the net
+// (limited face fluxes, learned-face weights) is P::finish, in FP32. `wblob`: every half net's weights, BF16, each
+// layer's K x N matrix in the core layout (rows = inputs); `wf`: the nets' FP32 parameters (shift, scale, biases,
+// output scale). A wait that gives up sets a.err, and the kernel leaves through its normal exit (tensor memory freed).
+template <class P>
+__device__ __forceinline__ void fe_net_pass(const FePassArgs& a, const unsigned short* wblob, const float* wf)
+{
+    extern __shared__ __align__(128) float fe_sm[];
+    unsigned char* sm = reinterpret_cast<unsigned char*>(fe_sm);
+    unsigned char* weights = sm + P::EC * P::A_BYTES;
+    fe_u64* bar = reinterpret_cast<fe_u64*>(weights + P::W_BYTES);
+    unsigned* tslot = reinterpret_cast<unsigned*>(bar + 1);
+    const int t = threadIdx.x;
+    const int warp = t >> 5;
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(reinterpret_cast<const unsigned char*>(wblob) + P::WOFF);
+        uint4* dst = reinterpret_cast<uint4*>(weights);
+        for (int i = t; i < static_cast<int>(P::W_BYTES / 16); i += 128) dst[i] = src[i];
+    }
+    if (t == 0) {
+        fe_mbar_init(bar, 1);
+        fe_fence_mbar_init();
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(fe_smem(tslot)), "r"(P::TCOLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fe_fence_proxy_async();
+    fe_tc_before();
+    __syncthreads();
+    fe_tc_after();
+    const unsigned tbase = *tslot;
+    const unsigned lane = tbase + (static_cast<unsigned>(warp * 32) << 16);
+    const unsigned s0 = fe_smem(sm);
+    const unsigned w0 = fe_smem(weights);
+    FePlainCtx<P> c;
+    c.src = a.src;
+    c.dt = a.dt;
+    const fe_u64 cells = static_cast<fe_u64>(P::NX) * P::NY * P::NZ;
+    const fe_u64 tiles = (cells + 127) / 128;
+    unsigned phase = 0;
+    bool ok = true;
+    for (fe_u64 tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const fe_u64 cell = tile * 128 + static_cast<fe_u64>(t);
+        const bool valid = cell < cells;
+        const fe_u64 at = valid ? cell : cells - 1;
+        const int x = static_cast<int>(at % P::NX);
+        const int y = static_cast<int>((at / P::NX) % P::NY);
+        const int z = static_cast<int>(at / (static_cast<fe_u64>(P::NX) * P::NY));
+        float yv[P::E][P::NOUT];
+#pragma unroll 1
+        for (int ch = 0; ch < P::E && ok; ch += P::EC) {
+            const int count = P::E - ch < P::EC ? P::E - ch : P::EC;
+            // Layer 0's operands: the inputs, shifted and scaled (FP32), then BF16; zeros past the net's inputs.
+            for (int ee = 0; ee < count; ++ee) {
+                float xin[P::KP0];
+#pragma unroll
+                for (int i = 0; i < P::KP0; ++i) xin[i] = 0.f;
+                P::input(c, x, y, z, ch + ee, xin);
+#pragma unroll
+                for (int i = 0; i < P::NIN; ++i) xin[i] = (xin[i] - wf[P::SHIFT + i]) * wf[P::SCALE + i];
+#pragma unroll
+                for (int c0 = 0; c0 < P::KP0; c0 += 8) fe_tc_put8(sm + ee * P::A_BYTES, t, c0, xin + c0);
+            }
+#pragma unroll
+            for (int l = 0; l < P::L; ++l) {
+                fe_fence_proxy_async();
+                fe_tc_ld_wait();
+                fe_tc_before();
+                __syncthreads();
+                if (t == 0) {
+                    fe_tc_after();
+                    for (int ee = 0; ee < count; ++ee) {
+                        for (int ks = 0; ks < P::kp(l) / 16; ++ks) {
+                            fe_tc_mma(tbase + static_cast<unsigned>(ee * P::NMAX),
+                                fe_tc_sdesc(s0 + ee * P::A_BYTES + ks * 2 * 2048, 2048, 128),
+                                fe_tc_sdesc(w0 + P::wb(l) + ks * 2 * 128, 128, (P::kp(l) / 8) * 128), fe_tc_idesc(128, P::np(l)), ks > 0);
+                        }
+                    }
+                    fe_tc_commit(bar);
+                }
+                const bool mine = fe_mbar_wait(bar, phase, 1u << 22);
+                ok = __syncthreads_and(mine) != 0;
+                fe_tc_after();
+                if (!ok) {
+                    if (t == 0) atomicOr(a.err, FE_ERR_MBAR_TIMEOUT);
+                    break;
+                }
+                phase ^= 1u;
+                for (int ee = 0; ee < count; ++ee) {
+#pragma unroll
+                    for (int c0 = 0; c0 < P::np(l); c0 += 16) {
+                        float v[16];
+                        fe_tc_ld16(lane + static_cast<unsigned>(ee * P::NMAX + c0), v);
+                        fe_tc_ld_wait();
+                        if (l + 1 < P::L) {
+#pragma unroll
+                            for (int i = 0; i < 16; ++i) v[i] = c0 + i < P::no(l) ? P::act(v[i] + wf[P::bias(l) + c0 + i]) : 0.f;
+                            fe_tc_put8(sm + ee * P::A_BYTES, t, c0, v);
+                            fe_tc_put8(sm + ee * P::A_BYTES, t, c0 + 8, v + 8);
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < 16; ++i) {
+                                if (c0 + i < P::NOUT) yv[ch + ee][c0 + i] = (v[i] + wf[P::bias(l) + c0 + i]) * wf[P::OSCALE];
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        if (ok && valid) a.out[0][cell] = P::finish(c, x, y, z, yv);
+    }
+    if (!ok) {
+        // The MMAs whose wait gave up may still run: one more bounded wait before their tensor memory is freed.
+        fe_mbar_wait(bar, phase, 1u << 22);
+    }
+    fe_tc_ld_wait();
+    fe_tc_before();
+    __syncthreads();
+    if (warp == 0) {
+        fe_tc_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(P::TCOLS) : "memory");
+    }
+}
+
 #endif // device code
 
 #endif // FE_DEVICE_CUH
