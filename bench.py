@@ -691,7 +691,9 @@ def profile_case(name):
     heat        the heat law on 512^3 (the bench's lattice; inputs larger than L2), 3 steps: the generated gather;
     heston      36 options on 512 x 256, 16 Douglas steps, split (16, 4, 512): the cluster kernel;
     corrector   3 training steps, one gradient and one guarded apply on 256 x 32 x 32 cells: the tcgen05 kernels;
-    multifield  the 43-term law on 128^3, 3 steps: its generated passes."""
+    multifield  the 43-term law on 128^3, 3 steps: its generated passes;
+    nets        the learned-flux and learned-conduction laws (tests/laws/nets_flux.law, nets_ldiffuse.law) on
+                128 x 128 x 64, 3 steps each with fp32 nets, then with the nets declared half: the tcgen05 net stages."""
     import numpy as np
     import torch
     if name == "heston":
@@ -739,6 +741,25 @@ def profile_case(name):
         s.sync()
         print(json.dumps({"case": name, "violations": len(s.violations())}))
         s.close()
+    elif name == "nets":
+        from fieldcuda.solver import Solver
+        os.chdir(ROOT)  # the laws' weight files are repository paths
+        rng = np.random.default_rng(5)
+        n, nz = 128, 64
+        out = {}
+        for law in ("nets_flux.law", "nets_ldiffuse.law"):
+            text = open(os.path.join("tests", "laws", law)).read()
+            for form, t in (("fp32", text), ("half", text.replace(" file ", " half file "))):
+                s = Solver(t, n, n, nz, 0.5, law)
+                s.set_field("T", (290 + 600 * rng.random((nz, n, n))).astype(np.float32))
+                if "fuel" in s.field_names:
+                    s.set_field("fuel", rng.random((nz, n, n)).astype(np.float32))
+                for _ in range(3):
+                    s.step(0.02)
+                s.sync()
+                out[f"{law}:{form}"] = len(s.violations())
+                s.close()
+        print(json.dumps({"case": name, "violations": out}))
     else:
         raise SystemExit(f"no profile case {name!r}")
 
@@ -755,7 +776,7 @@ def main():
     ap.add_argument("--no-multifield", action="store_true", help="skip the 43-term multi-field law section")
     ap.add_argument("--no-calibration", action="store_true", help="skip the adjoint calibration section")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-correction section")
-    ap.add_argument("--profile-case", default="", help="run one small case for ncu (heat, heston, corrector, multifield) and exit")
+    ap.add_argument("--profile-case", default="", help="run one small case for ncu (heat, heston, corrector, multifield, nets) and exit")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)

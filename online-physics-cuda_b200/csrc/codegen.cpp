@@ -980,7 +980,7 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
         const law::NetDecl& net = law_.nets[static_cast<std::size_t>(in.index)];
         const NetAt& na = net_at_[static_cast<std::size_t>(in.index)];
         const int layers = net.layers();
-        std::vector<int> kp, np, no, wb, bias;
+        std::vector<int> kp, np, no, wb;
         int wbytes = 0, nmax = 16, kmax = 16;
         for (int l = 0; l < layers; ++l) {
             const int ni = net.sizes[static_cast<std::size_t>(l)];
@@ -993,15 +993,15 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
             np.push_back(pad16(o));
             no.push_back(o);
             wb.push_back(wbytes);
-            bias.push_back(static_cast<int>(na.w0 + net.weight_offset(l) + static_cast<std::size_t>(ni) * o));
             wbytes += pad16(ni) * pad16(o) * 2;
             nmax = std::max(nmax, pad16(o));
             kmax = std::max(kmax, pad16(ni));
         }
         int e = 1, nin = static_cast<int>(in.args.size());
+        const std::size_t m = in.op == Op::Flux ? in.args.size() - 2 : 0;
         if (in.op == Op::Flux) {
             e = 12;
-            nin = 2 * (static_cast<int>(in.args.size()) - 2);
+            nin = 2 * static_cast<int>(m);
         } else if (in.op == Op::LDiffuse) {
             e = 12;
             nin = 5;
@@ -1011,7 +1011,11 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
             why = "net '" + net.name + "' does not fit its op";
             return false;
         }
-        const int ec = std::max(1, std::min(e, 128 / nmax));
+        // Evaluations a chunk: whole faces (pairs), as many as 64 accumulator columns hold (at least one face), so that
+        // eight CTAs an SM find tensor memory when the net is at most 32 wide.
+        const int pair = e == 1 ? 1 : 2;
+        int ec = e == 1 ? 1 : std::max(2, (64 / nmax) / 2 * 2);
+        while (e % ec != 0) ec -= pair;
         int tcols = 32;
         while (tcols < ec * nmax) tcols *= 2;
         const int per_sm = std::min(8, 512 / tcols);
@@ -1042,15 +1046,19 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
             for (std::size_t k = 0; k < v.size(); ++k) f << "if (l == " << k << ") return " << v[k] << "; ";
             f << "return 0; }\n";
         };
+        auto table = [&](const std::vector<float>& v, std::size_t size) {
+            std::string t = "{";
+            for (std::size_t k = 0; k < size; ++k) t += (k ? ", " : "") + literal(k < v.size() ? v[k] : 0.0f);
+            return t + "}";
+        };
         // The face f (0..5: -x, +x, -y, +y, -z, +z) of a cell: its lower cell i and upper cell j (clamped: a face past
         // the lattice's edge is never used), and whether it is open.
         f << "__device__ __forceinline__ void face_cells(int f, int x, int y, int z, int& ix, int& iy, int& iz, int& jx, int& jy, int& jz) {\n"
           << "    const int ax = f >> 1; ix = x; iy = y; iz = z;\n"
           << "    if ((f & 1) == 0) { ix = fe_ex(x - (ax == 0)); iy = fe_ey(y - (ax == 1)); iz = fe_ez(z - (ax == 2)); }\n"
           << "    jx = fe_ex(ix + (ax == 0)); jy = fe_ey(iy + (ax == 1)); jz = fe_ez(iz + (ax == 2)); }\n"
-          << "__device__ __forceinline__ bool face_open(int f, int x, int y, int z) {\n"
-          << "    const int ax = f >> 1; const int q = ax == 0 ? x : (ax == 1 ? y : z); const int n = ax == 0 ? NX : (ax == 1 ? NY : NZ);\n"
-          << "    return (f & 1) ? q + 1 < n : q > 0; }\n";
+          << "__device__ __forceinline__ unsigned faces_open(int x, int y, int z) {\n"
+          << "    return (x > 0 ? 1u : 0u) | (x + 1 < NX ? 2u : 0u) | (y > 0 ? 4u : 0u) | (y + 1 < NY ? 8u : 0u) | (z > 0 ? 16u : 0u) | (z + 1 < NZ ? 32u : 0u); }\n";
         if (in.op == Op::LDiffuse) {
             // The window F[i-1] F[i] | F[j] F[j+1] of the face between i = (x, y, z) and its +AX neighbour j (edge
             // cells repeat), and k's face value (the harmonic mean, in double): the fp32 form's arithmetic.
@@ -1063,10 +1071,6 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
               << "; w[3] = " << arg(1, "px", "py", "pz") << ";\n"
               << "    const double ka = " << arg(0, "x", "y", "z") << ", kb = " << arg(0, "jx", "jy", "jz") << ";\n"
               << "    kf = static_cast<float>((ka + kb) > 0.0 ? 2.0 * ka * kb / (ka + kb) : 0.0); }\n"
-              << "template <class C> __device__ __forceinline__ void face_window(const C& c, int f, int x, int y, int z, float* w, float& kf) {\n"
-              << "    int ix, iy, iz, jx, jy, jz; face_cells(f, x, y, z, ix, iy, iz, jx, jy, jz);\n"
-              << "    const int ax = f >> 1;\n"
-              << "    if (ax == 0) window<0>(c, ix, iy, iz, w, kf); else if (ax == 1) window<1>(c, ix, iy, iz, w, kf); else window<2>(c, ix, iy, iz, w, kf); }\n"
               << "__device__ __forceinline__ float after_net(const float* yw, const float* w, float kf) {\n"
               << "    const float mean = 0.25f * (yw[0] + yw[1] + yw[2] + yw[3]);\n"
               << "    const float base[4] = {0.f, -1.f, 1.f, 0.f}; float acc = 0.f;\n"
@@ -1075,60 +1079,88 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
         }
         f << "struct P {\n"
           << "    static constexpr int NX = ::NX, NY = ::NY, NZ = ::NZ;\n"
-          << "    static constexpr int E = " << e << ", EC = " << ec << ", NIN = " << nin << ", NOUT = " << nout << ", L = " << layers
-          << ", NMAX = " << nmax << ", KP0 = " << kp[0] << ";\n"
+          << "    static constexpr int E = " << e << ", EC = " << ec << ", PAIR = " << pair << ", NIN = " << nin << ", NOUT = " << nout
+          << ", L = " << layers << ", NMAX = " << nmax << ", KP0 = " << kp[0] << ";\n"
           << "    static constexpr unsigned TCOLS = " << tcols << "u, A_BYTES = " << a_bytes << "u, W_BYTES = " << wbytes << "u, WOFF = " << na.bf16_bytes
           << "u;\n"
-          << "    static constexpr int SHIFT = " << na.shift << ", SCALE = " << na.scale << ", OSCALE = " << na.oscale << ";\n";
+          << "    static constexpr float OSCALE = " << literal(net.out_scale) << ";\n";
         fn("int", "kp", kp);
         fn("int", "np", np);
         fn("int", "no", no);
         fn("unsigned", "wb", wb);
-        fn("int", "bias", bias);
-        f << "    static __device__ __forceinline__ float act(float v) { return fe_act" << in.index << "(v); }\n";
-        f << "    template <class C> static __device__ __forceinline__ void input(const C& c, int x, int y, int z, int e, float* xin) {\n";
+        // The net's FP32 parameters as literals (fixed when the law is created): the inputs' shift and scale, the biases.
+        f << "    static __device__ __forceinline__ float shift(int i) { constexpr float v[] = " << table(net.in_shift, static_cast<std::size_t>(kp[0]))
+          << "; return v[i]; }\n"
+          << "    static __device__ __forceinline__ float scale(int i) { constexpr float v[] = " << table(net.in_scale, static_cast<std::size_t>(kp[0]))
+          << "; return v[i]; }\n"
+          << "    static __device__ __forceinline__ float bias(int l, int o) {\n";
+        for (int l = 0; l < layers; ++l) {
+            const std::size_t off = net.weight_offset(l) + static_cast<std::size_t>(net.sizes[static_cast<std::size_t>(l)]) * no[static_cast<std::size_t>(l)];
+            std::vector<float> b(net.weights.begin() + static_cast<std::ptrdiff_t>(off),
+                net.weights.begin() + static_cast<std::ptrdiff_t>(off) + no[static_cast<std::size_t>(l)]);
+            f << "        if (l == " << l << ") { constexpr float v[] = " << table(b, static_cast<std::size_t>(np[static_cast<std::size_t>(l)])) << "; return v[o]; }\n";
+        }
+        f << "        return 0.f; }\n";
+        const std::string act = net.act == "tanh" ? "fe_tanh_approx(v)" : net.act == "relu" ? "(v > 0.f ? v : 0.f)" : net.act == "silu" ? "fe_silu_approx(v)" : "v";
+        f << "    static __device__ __forceinline__ float act(float v) { return " << act << "; }\n";
         if (in.op == Op::Mlp) {
-            for (std::size_t k = 0; k < in.args.size(); ++k) f << "        xin[" << k << "] = " << arg(k, "x", "y", "z") << ";\n";
+            f << "    struct Keep { float x[" << nin << "]; };\n"
+              << "    template <class C> static __device__ __forceinline__ void prepare(const C& c, int x, int y, int z, Keep& k) {\n";
+            for (std::size_t q = 0; q < in.args.size(); ++q) f << "        k.x[" << q << "] = " << arg(q, "x", "y", "z") << ";\n";
             f << "    }\n"
-              << "    template <class C> static __device__ __forceinline__ float finish(const C&, int, int, int, const float (*yv)[NOUT]) { return yv[0][0]; }\n";
+              << "    static __device__ __forceinline__ void input(const Keep& k, int, float* xin) {\n"
+              << "#pragma unroll\n        for (int i = 0; i < NIN; ++i) xin[i] = k.x[i]; }\n"
+              << "    static __device__ __forceinline__ void take(const Keep&, int, const float* y0, const float*, float& o) { o = y0[0]; }\n"
+              << "    static __device__ __forceinline__ float result(float o) { return o; }\n";
         } else if (in.op == Op::Flux) {
-            const std::size_t m = in.args.size() - 2;
             char bounds[96];
             std::snprintf(bounds, sizeof(bounds), "%.17g, %.17g", at(in.args[m]).number, at(in.args[m + 1]).number);
-            f << "        int ix, iy, iz, jx, jy, jz; face_cells(e >> 1, x, y, z, ix, iy, iz, jx, jy, jz);\n"
-              << "        if (e & 1) { int t = ix; ix = jx; jx = t; t = iy; iy = jy; jy = t; t = iz; iz = jz; jz = t; }\n";
-            for (std::size_t k = 0; k < m; ++k) {
-                f << "        xin[" << k << "] = " << arg(k, "ix", "iy", "iz") << "; xin[" << m + k << "] = " << arg(k, "jx", "jy", "jz") << ";\n";
-            }
-            f << "    }\n"
-              << "    template <class C> static __device__ __forceinline__ float finish(const C& c, int x, int y, int z, const float (*yv)[NOUT]) {\n"
-              << "        float o = 0.f;\n"
-              << "#pragma unroll\n        for (int f = 0; f < 6; ++f) {\n"
-              << "            if (!face_open(f, x, y, z)) continue;\n"
+            // The cell's own values and its six neighbours' (a closed face's neighbour is the cell itself).
+            f << "    struct Keep { float cen[" << m << "]; float nb[6][" << m << "]; unsigned open; float dt; };\n"
+              << "    template <class C> static __device__ __forceinline__ void prepare(const C& c, int x, int y, int z, Keep& k) {\n";
+            for (std::size_t q = 0; q < m; ++q) f << "        k.cen[" << q << "] = " << arg(q, "x", "y", "z") << ";\n";
+            f << "#pragma unroll\n        for (int f = 0; f < 6; ++f) {\n"
               << "            int ix, iy, iz, jx, jy, jz; face_cells(f, x, y, z, ix, iy, iz, jx, jy, jz);\n"
-              << "            const float g = fe_limit_face(0.5f * (yv[2 * f][0] - yv[2 * f + 1][0]), " << arg(0, "ix", "iy", "iz") << ", "
-              << arg(0, "jx", "jy", "jz") << ", " << bounds << ", c.dt);\n"
-              << "            if (f & 1) o -= g; else o += g;\n"
-              << "        }\n"
-              << "        return o / FE_H; }\n";
+              << "            const int nx = (f & 1) ? jx : ix, ny = (f & 1) ? jy : iy, nz = (f & 1) ? jz : iz;\n";
+            for (std::size_t q = 0; q < m; ++q) f << "            k.nb[f][" << q << "] = " << arg(q, "nx", "ny", "nz") << ";\n";
+            f << "        }\n"
+              << "        k.open = faces_open(x, y, z); k.dt = c.dt; }\n"
+              // Way 0 sees (i, j), way 1 (j, i); i is the face's lower cell.
+              << "    static __device__ __forceinline__ void input(const Keep& k, int e, float* xin) {\n"
+              << "        const int f = e >> 1; const bool up = (f & 1) != 0; const bool way = (e & 1) != 0;\n"
+              << "        const float* i = up ? k.cen : k.nb[f]; const float* j = up ? k.nb[f] : k.cen;\n"
+              << "#pragma unroll\n        for (int q = 0; q < " << m << "; ++q) { xin[q] = way ? j[q] : i[q]; xin[" << m << " + q] = way ? i[q] : j[q]; } }\n"
+              << "    static __device__ __forceinline__ void take(const Keep& k, int e, const float* y0, const float* y1, float& o) {\n"
+              << "        const int f = e >> 1; const bool up = (f & 1) != 0;\n"
+              << "        if (((k.open >> f) & 1u) == 0u) return;\n"
+              << "        const float fi = up ? k.cen[0] : k.nb[f][0], fj = up ? k.nb[f][0] : k.cen[0];\n"
+              << "        const float g = fe_limit_face(0.5f * (y0[0] - y1[0]), fi, fj, " << bounds << ", k.dt);\n"
+              << "        if (up) o -= g; else o += g; }\n"
+              << "    static __device__ __forceinline__ float result(float o) { return o / FE_H; }\n";
         } else {
-            f << "        float w[4], kf; face_window(c, e >> 1, x, y, z, w, kf);\n"
-              << "        if (e & 1) { float t = w[0]; w[0] = w[3]; w[3] = t; t = w[1]; w[1] = w[2]; w[2] = t; }\n"
+            f << "    struct Keep { float w[6][4]; float kf[6]; unsigned open; float dt; };\n"
+              << "    template <class C> static __device__ __forceinline__ void prepare(const C& c, int x, int y, int z, Keep& k) {\n"
+              << "#pragma unroll\n        for (int f = 0; f < 6; ++f) {\n"
+              << "            int ix, iy, iz, jx, jy, jz; face_cells(f, x, y, z, ix, iy, iz, jx, jy, jz);\n"
+              << "            if ((f >> 1) == 0) window<0>(c, ix, iy, iz, k.w[f], k.kf[f]);\n"
+              << "            else if ((f >> 1) == 1) window<1>(c, ix, iy, iz, k.w[f], k.kf[f]);\n"
+              << "            else window<2>(c, ix, iy, iz, k.w[f], k.kf[f]);\n"
+              << "        }\n"
+              << "        k.open = faces_open(x, y, z); k.dt = c.dt; }\n"
+              // Way 1 is the mirrored window: the same centre and spread, so its inputs are way 0's reversed.
+              << "    static __device__ __forceinline__ void input(const Keep& k, int e, float* xin) {\n"
+              << "        const int f = e >> 1; const float* w = k.w[f];\n"
               << "        const float centre = 0.5f * (w[1] + w[2]); float spread = 1e-6f;\n"
               << "#pragma unroll\n        for (int q = 0; q < 4; ++q) spread = fmaxf(spread, fabsf(w[q] - centre));\n"
-              << "#pragma unroll\n        for (int q = 0; q < 4; ++q) xin[q] = (w[q] - centre) / spread;\n"
-              << "        xin[4] = kf * c.dt / (FE_H * FE_H);\n"
-              << "    }\n"
-              << "    template <class C> static __device__ __forceinline__ float finish(const C& c, int x, int y, int z, const float (*yv)[NOUT]) {\n"
-              << "        float o = 0.f;\n"
-              << "#pragma unroll\n        for (int f = 0; f < 6; ++f) {\n"
-              << "            if (!face_open(f, x, y, z)) continue;\n"
-              << "            float w[4], kf; face_window(c, f, x, y, z, w, kf);\n"
-              << "            const float mirror[4] = {w[3], w[2], w[1], w[0]};\n"
-              << "            const float g = 0.5f * (after_net(yv[2 * f], w, kf) - after_net(yv[2 * f + 1], mirror, kf));\n"
-              << "            if (f & 1) o -= g; else o += g;\n"
-              << "        }\n"
-              << "        return o / FE_H; }\n";
+              << "#pragma unroll\n        for (int q = 0; q < 4; ++q) xin[(e & 1) ? 3 - q : q] = (w[q] - centre) / spread;\n"
+              << "        xin[4] = k.kf[f] * k.dt / (FE_H * FE_H); }\n"
+              << "    static __device__ __forceinline__ void take(const Keep& k, int e, const float* y0, const float* y1, float& o) {\n"
+              << "        const int f = e >> 1; const bool up = (f & 1) != 0;\n"
+              << "        if (((k.open >> f) & 1u) == 0u) return;\n"
+              << "        const float* w = k.w[f]; const float mirror[4] = {w[3], w[2], w[1], w[0]};\n"
+              << "        const float g = 0.5f * (after_net(y0, w, k.kf[f]) - after_net(y1, mirror, k.kf[f]));\n"
+              << "        if (up) o -= g; else o += g; }\n"
+              << "    static __device__ __forceinline__ float result(float o) { return o / FE_H; }\n";
         }
         f << "};\n}\n";
         L.kind = Launch::Net;
@@ -1143,7 +1175,7 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
         L.per_sm = per_sm;
         L.kernel = "fe_net_" + tag;
         f << "extern \"C\" __global__ void __launch_bounds__(128) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_net_pass<" << ns
-          << "::P>(a, FE_NETB, FE_NET); }\n";
+          << "::P>(a, FE_NETB); }\n";
         out_ << f.str();
         return true;
     }

@@ -1049,14 +1049,15 @@ __device__ __forceinline__ void fe_tc_put8(unsigned char* tile, int r, int c0, c
 // A net op whose net is declared `half` (the reference's tensor-core nets, CudaNet.cpp:175-277), as one stage kernel:
 // 128 threads, thread t owns cell t of a 128-cell tile and row / tensor-memory lane t, persistent over tiles. A cell
 // needs P::E evaluations of the net (mlp 1; flux and ldiffuse 12: six faces, both ways round); P::EC of them at a time
-// are 128-row tiles in shared memory, and each layer is P::EC M = 128 MMAs (K = 16 a step) into their own accumulator
-// columns. Between layers every thread reads its row back, adds the FP32 bias, applies the activation and writes the
-// next layer's BF16 operand over the last one (whose MMAs have completed). The op's own arithmetic around the net
-// (limited face fluxes, learned-face weights) is P::finish, in FP32. `wblob`: every half net's weights, BF16, each
-// layer's K x N matrix in the core layout (rows = inputs); `wf`: the nets' FP32 parameters (shift, scale, biases,
-// output scale). A wait that gives up sets a.err, and the kernel leaves through its normal exit (tensor memory freed).
+// (whole faces) are 128-row tiles in shared memory, and each layer is P::EC M = 128 MMAs (K = 16 a step) into their
+// own accumulator columns. Between layers every thread reads its row back, adds the bias, applies the activation and
+// writes the next layer's BF16 operand over the last one (whose MMAs have completed). P::prepare gathers what a cell's
+// evaluations read once (its arguments, or each face's two sides or window); P::take folds a face's two evaluations
+// (or mlp's one) into the cell's value, in FP32, as soon as they are out. `wblob`: every half net's weights, BF16,
+// each layer's K x N matrix in the core layout (rows = inputs). A wait that gives up sets a.err and the rest of the
+// tile's MMAs are skipped; the kernel leaves through its normal exit (tensor memory freed).
 template <class P>
-__device__ __forceinline__ void fe_net_pass(const FePassArgs& a, const unsigned short* wblob, const float* wf)
+__device__ __forceinline__ void fe_net_pass(const FePassArgs& a, const unsigned short* wblob)
 {
     extern __shared__ __align__(128) float fe_sm[];
     unsigned char* sm = reinterpret_cast<unsigned char*>(fe_sm);
@@ -1100,47 +1101,50 @@ __device__ __forceinline__ void fe_net_pass(const FePassArgs& a, const unsigned 
         const int x = static_cast<int>(at % P::NX);
         const int y = static_cast<int>((at / P::NX) % P::NY);
         const int z = static_cast<int>(at / (static_cast<fe_u64>(P::NX) * P::NY));
-        float yv[P::E][P::NOUT];
-#pragma unroll 1
-        for (int ch = 0; ch < P::E && ok; ch += P::EC) {
-            const int count = P::E - ch < P::EC ? P::E - ch : P::EC;
+        typename P::Keep keep;
+        P::prepare(c, x, y, z, keep);
+        float o = 0.f;
+#pragma unroll
+        for (int ch = 0; ch < P::E; ch += P::EC) {
             // Layer 0's operands: the inputs, shifted and scaled (FP32), then BF16; zeros past the net's inputs.
-            for (int ee = 0; ee < count; ++ee) {
+#pragma unroll
+            for (int ee = 0; ee < P::EC; ++ee) {
                 float xin[P::KP0];
 #pragma unroll
                 for (int i = 0; i < P::KP0; ++i) xin[i] = 0.f;
-                P::input(c, x, y, z, ch + ee, xin);
+                P::input(keep, ch + ee, xin);
 #pragma unroll
-                for (int i = 0; i < P::NIN; ++i) xin[i] = (xin[i] - wf[P::SHIFT + i]) * wf[P::SCALE + i];
+                for (int i = 0; i < P::NIN; ++i) xin[i] = (xin[i] - P::shift(i)) * P::scale(i);
 #pragma unroll
                 for (int c0 = 0; c0 < P::KP0; c0 += 8) fe_tc_put8(sm + ee * P::A_BYTES, t, c0, xin + c0);
             }
+            float yout[P::EC][P::NOUT];
 #pragma unroll
             for (int l = 0; l < P::L; ++l) {
-                fe_fence_proxy_async();
-                fe_tc_ld_wait();
-                fe_tc_before();
-                __syncthreads();
-                if (t == 0) {
-                    fe_tc_after();
-                    for (int ee = 0; ee < count; ++ee) {
-                        for (int ks = 0; ks < P::kp(l) / 16; ++ks) {
-                            fe_tc_mma(tbase + static_cast<unsigned>(ee * P::NMAX),
-                                fe_tc_sdesc(s0 + ee * P::A_BYTES + ks * 2 * 2048, 2048, 128),
-                                fe_tc_sdesc(w0 + P::wb(l) + ks * 2 * 128, 128, (P::kp(l) / 8) * 128), fe_tc_idesc(128, P::np(l)), ks > 0);
+                if (ok) {
+                    fe_fence_proxy_async();
+                    fe_tc_ld_wait();
+                    fe_tc_before();
+                    __syncthreads();
+                    if (t == 0) {
+                        fe_tc_after();
+                        for (int ee = 0; ee < P::EC; ++ee) {
+                            for (int ks = 0; ks < P::kp(l) / 16; ++ks) {
+                                fe_tc_mma(tbase + static_cast<unsigned>(ee * P::NMAX),
+                                    fe_tc_sdesc(s0 + ee * P::A_BYTES + ks * 2 * 2048, 2048, 128),
+                                    fe_tc_sdesc(w0 + P::wb(l) + ks * 2 * 128, 128, (P::kp(l) / 8) * 128), fe_tc_idesc(128, P::np(l)), ks > 0);
+                            }
                         }
+                        fe_tc_commit(bar);
                     }
-                    fe_tc_commit(bar);
+                    const bool mine = fe_mbar_wait(bar, phase, 1u << 22);
+                    ok = __syncthreads_and(mine) != 0;
+                    fe_tc_after();
+                    if (ok) phase ^= 1u;
+                    else if (t == 0) atomicOr(a.err, FE_ERR_MBAR_TIMEOUT);
                 }
-                const bool mine = fe_mbar_wait(bar, phase, 1u << 22);
-                ok = __syncthreads_and(mine) != 0;
-                fe_tc_after();
-                if (!ok) {
-                    if (t == 0) atomicOr(a.err, FE_ERR_MBAR_TIMEOUT);
-                    break;
-                }
-                phase ^= 1u;
-                for (int ee = 0; ee < count; ++ee) {
+#pragma unroll
+                for (int ee = 0; ee < P::EC && ok; ++ee) {
 #pragma unroll
                     for (int c0 = 0; c0 < P::np(l); c0 += 16) {
                         float v[16];
@@ -1148,20 +1152,22 @@ __device__ __forceinline__ void fe_net_pass(const FePassArgs& a, const unsigned 
                         fe_tc_ld_wait();
                         if (l + 1 < P::L) {
 #pragma unroll
-                            for (int i = 0; i < 16; ++i) v[i] = c0 + i < P::no(l) ? P::act(v[i] + wf[P::bias(l) + c0 + i]) : 0.f;
+                            for (int i = 0; i < 16; ++i) v[i] = c0 + i < P::no(l) ? P::act(v[i] + P::bias(l, c0 + i)) : 0.f;
                             fe_tc_put8(sm + ee * P::A_BYTES, t, c0, v);
                             fe_tc_put8(sm + ee * P::A_BYTES, t, c0 + 8, v + 8);
                         } else {
 #pragma unroll
                             for (int i = 0; i < 16; ++i) {
-                                if (c0 + i < P::NOUT) yv[ch + ee][c0 + i] = (v[i] + wf[P::bias(l) + c0 + i]) * wf[P::OSCALE];
+                                if (c0 + i < P::NOUT) yout[ee][c0 + i] = (v[i] + P::bias(l, c0 + i)) * P::OSCALE;
                             }
                         }
                     }
                 }
             }
+#pragma unroll
+            for (int ee = 0; ee < P::EC; ee += P::PAIR) P::take(keep, ch + ee, yout[ee], yout[ee + P::PAIR - 1], o);
         }
-        if (ok && valid) a.out[0][cell] = P::finish(c, x, y, z, yv);
+        if (ok && valid) a.out[0][cell] = P::result(o);
     }
     if (!ok) {
         // The MMAs whose wait gave up may still run: one more bounded wait before their tensor memory is freed.
@@ -1175,6 +1181,16 @@ __device__ __forceinline__ void fe_net_pass(const FePassArgs& a, const unsigned 
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(P::TCOLS) : "memory");
     }
 }
+
+// Activations of the tensor-core nets, whose layers are BF16 (8 significant bits): the hardware's approximate tanh
+// and exponential are well inside that.
+__device__ __forceinline__ float fe_tanh_approx(float v)
+{
+    float r;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(v));
+    return r;
+}
+__device__ __forceinline__ float fe_silu_approx(float v) { return __fdividef(v, 1.f + __expf(-v)); }
 
 #endif // device code
 
