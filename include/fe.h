@@ -231,6 +231,29 @@ int fe_law_stream(const fe_law* law, void** stream);
 /* Device time of `launches` back-to-back launches of term `term`'s fused gather pass (the roofline's kernel). */
 int fe_law_time_gather(fe_law* law, int term, int launches, float* ms);
 
+/* ---- reverse mode through a law's steps ------------------------------------------------------------------------------
+ * N steps of one term of a law and their vector-Jacobian product, natively (replaces the reference's lawc --vjp driver,
+ * tools/lawc/main.cpp:274-361, which keeps every state on the host and uploads one before each adjoint step). The handle
+ * holds two law handles (fe_vjp_laws): the primal law, and its adjoint law (fe_law_adjoint: X__adj the cotangent of
+ * field or param X). The differentiated term must be the only one that moves anything, one substep a step.
+ *   fe_vjp_forward: steps the primal `steps` times from its current fields, keeping every `every`-th state of its
+ *     moving fields on the device (every <= 0: ceil(sqrt(steps))); FE_EINVAL when the term took more than one substep,
+ *     FE_ELAW when a contract broke;
+ *   fe_vjp_backward: from the cotangents the caller put in the adjoint law's X__adj fields (the seeds; the adjoint law's
+ *     other fields are filled here), steps the adjoint law back over the forward's states, each segment recomputed
+ *     from its checkpoint; afterwards X__adj holds the cotangent of X at the forward's start, and the primal's fields
+ *     are left at a recomputed state;
+ *   fe_vjp_param_grad: a param's gradient, the FP64 sum of its cotangent field.
+ * Device memory: about (steps / every + every) copies of the moving fields. */
+typedef struct fe_vjp fe_vjp;
+int fe_vjp_create(const char* law_text, const char* term, int nx, int ny, int nz, double h, fe_vjp** out);
+void fe_vjp_destroy(fe_vjp* vjp);
+int fe_vjp_laws(fe_vjp* vjp, fe_law** primal, fe_law** adjoint);
+int fe_vjp_set_param(fe_vjp* vjp, const char* name, double value);
+int fe_vjp_forward(fe_vjp* vjp, double dt, int steps, int every);
+int fe_vjp_backward(fe_vjp* vjp);
+int fe_vjp_param_grad(fe_vjp* vjp, const char* param, double* grad);
+
 /* ---- batched Heston ADI: many options on uneven grids in one persistent launch -----------------------------------------
  * The reference prices a batch as the z-planes of one lattice, every option on the same grid (bench/finance.py:253-288,
  * bench/laws/heston_adi.law); here every option has its own grid and all are stepped by one persistent kernel of 8-CTA

@@ -154,6 +154,13 @@ SIGNATURES = {
     "fe_law_digest": (_i, [_p, _c.POINTER(_c.c_uint64)]),
     "fe_law_stream": (_i, [_p, _c.POINTER(_p)]),
     "fe_law_time_gather": (_i, [_p, _i, _i, _c.POINTER(_c.c_float)]),
+    "fe_vjp_create": (_i, [_cs, _cs, _i, _i, _i, _d, _c.POINTER(_p)]),
+    "fe_vjp_destroy": (None, [_p]),
+    "fe_vjp_laws": (_i, [_p, _c.POINTER(_p), _c.POINTER(_p)]),
+    "fe_vjp_set_param": (_i, [_p, _cs, _d]),
+    "fe_vjp_forward": (_i, [_p, _d, _i, _i]),
+    "fe_vjp_backward": (_i, [_p]),
+    "fe_vjp_param_grad": (_i, [_p, _cs, _c.POINTER(_d)]),
     "fe_heston_batch_create": (_i, [_c.POINTER(fe_heston_option), _i, _i, _i, _c.POINTER(_p)]),
     "fe_heston_batch_destroy": (None, [_p]),
     "fe_heston_batch_set_split": (_i, [_p, _i, _i, _i]),

@@ -11,8 +11,10 @@ the scripts that drive it (the bench drivers, tools/lawjax) run unchanged with t
 
 Scenes are the reference's text format (src/field/Scene.hpp:9-17): grid, law, fill, box, ball, noise, param; dumps
 are raw float32 per field plus meta.json (Scene.cpp:112-135). The solves run on the GPU; the reference's CPU solver is
-not part of this backend, so --backend cpu and --compare are refused, and so is --vjp (fieldcuda.adjoint is reverse
-mode). --learned runs the terms' learned schemes under guard (main.cpp:260): a learned step that breaks a contract is
+not part of this backend, so --backend cpu and --compare are refused. --vjp SEED_DIR differentiates one term (--term)
+over the steps (main.cpp:274-361): the scene is the forward's start, SEED_DIR holds the cotangents of its end
+(X__adj.bin, the dump format; a missing one is zero), and --dump DIR writes the cotangents of the start to DIR/adjoint;
+the driver is the native one (fe_vjp_*: states kept on the card every ceil(sqrt(N)) steps, not all on the host). --learned runs the terms' learned schemes under guard (main.cpp:260): a learned step that breaks a contract is
 undone and taken classically, and the undone steps are counted in --profile and --json as the reference counts them.
 """
 import argparse
@@ -148,6 +150,57 @@ def print_profile(solver, step_ms):
             print(f"    {name:<22} x{sub}{marks.get(how, '')}")
 
 
+def run_vjp(args, scene, text):
+    """--vjp: the scene's start stepped forward, then the seed cotangents stepped back; prints the reference's line."""
+    import torch
+    from . import _lib
+    from .adjoint import LawVJP
+    nx, ny, nz, h = scene.grid
+    try:
+        vjp = LawVJP(text, nx, ny, nz, h, term=args.term or None)
+    except _lib.FeError as e:
+        print(e, file=sys.stderr)
+        return 1
+    try:
+        for name, value in scene.params + [(n, float(v)) for n, v in args.param]:
+            vjp.set_param(name, value)
+        p = vjp.primal
+        inits = {n: p.field_info(n)["init"] for n in p.field_names}
+        for name, v in scene_fields(scene, p.field_names, inits).items():
+            p.set_field(name, v)
+        p.refresh_derived()
+        if args.init:
+            load_fields(p, args.init)
+            p.refresh_derived()
+        if not os.path.isdir(args.vjp):
+            raise ValueError(f"no seed at {args.vjp}")
+        seeds = {}
+        for name in vjp.state:
+            path = os.path.join(args.vjp, name + "__adj.bin")
+            if os.path.exists(path):
+                v = np.fromfile(path, np.float32)
+                if v.size != nx * ny * nz:
+                    raise ValueError(f"{path} holds {v.size} floats, the lattice {nx * ny * nz}")
+                seeds[name] = torch.tensor(v.reshape(nz, ny, nx), device="cuda")
+        t0 = time.perf_counter()
+        vjp.forward({}, args.dt, args.steps)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        vjp.backward(seeds)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+    except (ValueError, _lib.FeError) as e:
+        print(e, file=sys.stderr)
+        vjp.close()
+        return 1
+    term = args.term or vjp.primal.term_names[0]
+    print(f"vjp of '{term}' over {args.steps} steps on B200: forward {(t1 - t0) * 1e3:g} ms, backward {(t2 - t1) * 1e3:g} ms")
+    if args.dump:
+        dump_fields(vjp.adj, os.path.join(args.dump, "adjoint"))
+    vjp.close()
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="lawc", description="the law compiler and runner on the B200 backend")
     ap.add_argument("laws", nargs="*")
@@ -178,8 +231,7 @@ def main(argv=None):
     if args.backend not in ("cuda", "b200"):
         print(f"no {args.backend} backend here: this lawc runs the B200 backend only", file=sys.stderr)
         return 1
-    for flag, what in ((args.compare, "--compare (the reference's CPU solver is not part of this backend)"),
-                       (args.vjp, "--vjp (reverse mode is fieldcuda.adjoint)")):
+    for flag, what in ((args.compare, "--compare (the reference's CPU solver is not part of this backend)"),):
         if flag:
             print(f"not in this lawc: {what}", file=sys.stderr)
             return 2
@@ -238,6 +290,8 @@ def main(argv=None):
         return 0
 
     nx, ny, nz, h = scene.grid
+    if args.vjp:
+        return run_vjp(args, scene, text)
     try:
         s = Solver(text, nx, ny, nz, h, source)
     except _lib.FeError as e:

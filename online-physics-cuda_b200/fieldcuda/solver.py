@@ -42,8 +42,20 @@ class Solver:
         handle = ctypes.c_void_p()
         _lib.check(self._lib.fe_law_create(law_text.encode(), source_name.encode(), nx, ny, nz, float(h),
                                            ctypes.byref(handle)))
+        self._attach(handle, (nz, ny, nx), h, owned=True)
+
+    @classmethod
+    def borrow(cls, handle, shape, h):
+        """A view of a law handle another object owns (a VJP's primal or adjoint law): close() leaves it alone."""
+        s = cls.__new__(cls)
+        s._lib = _lib.lib()
+        s._attach(handle, shape, h, owned=False)
+        return s
+
+    def _attach(self, handle, shape, h, owned):
         self._h = handle
-        self.shape = (nz, ny, nx)
+        self._owned = owned
+        self.shape = tuple(shape)
         self.h = h
         self.respect_max_dt = True
         n = self._lib.fe_law_field_count(self._h)
@@ -62,7 +74,8 @@ class Solver:
     # ---- lifetime ------------------------------------------------------------------------------------------------
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:
-            self._lib.fe_law_destroy(self._h)
+            if self._owned:
+                self._lib.fe_law_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

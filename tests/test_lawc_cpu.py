@@ -49,7 +49,6 @@ def test_ir_outputs_and_refusals(tmp_path):
     assert "T__adj" in adj.read_text()
     assert lawc.main(["--backend", "cpu", law]) == 1
     assert lawc.main(["--compare", "--steps", "1", law]) == 2
-    assert lawc.main(["--vjp", "x", "--steps", "1", law]) == 2
     bad = tmp_path / "bad.scene"
     bad.write_text("grid 4 4 4 1\nsprinkle T 1\n")
     with pytest.raises(ValueError, match="unknown line 'sprinkle'"):

@@ -46,3 +46,43 @@ def test_learned_run_counts_the_undone_steps(cuda, tmp_path, monkeypatch, capsys
     assert "learned step(s) undone" in printed
     rc = lawc.main(["--scene", "tests/scenes/guarded.scene", "--steps", "5", "--dt", "0.3", "--json", str(js)])
     assert rc == 0 and json.loads(js.read_text())["fallbacks"] == 0
+
+
+def test_vjp_matches_the_oracle_reverse_pass(cuda, tmp_path, monkeypatch):
+    """lawc --vjp (the native checkpointed driver) against the oracle keeping every state and running the same adjoint
+    law back over them, as the reference's lawc --vjp does."""
+    from fieldcuda import _lib, lawc
+    from fieldcuda.adjoint import adjoint_law
+    from oracle import law_cpu
+    monkeypatch.chdir(ROOT)
+    scene = lawc.load_scene("tests/scenes/heat_vjp.scene")
+    nx, ny, nz, h = scene.grid
+    law = open("tests/laws/heat.law").read()
+    steps, dt = 12, 0.4 * h * h / 6.0 * 0.9
+    rng = np.random.default_rng(11)
+    seed = rng.normal(size=(nz, ny, nx)).astype(np.float32)
+    (tmp_path / "seed").mkdir()
+    seed.tofile(tmp_path / "seed" / "T__adj.bin")
+    rc = lawc.main(["--scene", "tests/scenes/heat_vjp.scene", "--steps", str(steps), "--dt", repr(dt), "--vjp",
+                    str(tmp_path / "seed"), "--dump", str(tmp_path / "out")])
+    assert rc == 0
+    got = np.fromfile(tmp_path / "out" / "adjoint" / "T__adj.bin", np.float32).reshape(nz, ny, nx).astype(np.float64)
+
+    def solver(text, fields):
+        ir = json.loads(_lib.text_call("fe_law_ir_json", text.encode()))
+        s = law_cpu.Solver(law_cpu.Law(ir), (nz, ny, nx), h)
+        for k, v in fields.items():
+            s.fields[k] = np.asarray(v, law_cpu.F32).copy()
+        return s
+    start = lawc.scene_fields(scene, ["T"], {"T": 0.0})
+    o = solver(law, start)
+    states = []
+    for _ in range(steps):
+        states.append(o.fields["T"].copy())
+        o.step(dt)
+    a = solver(adjoint_law(law), dict(start, T__adj=seed))
+    for s in range(steps - 1, -1, -1):
+        a.fields["T"] = states[s]
+        a.step(dt)
+    want = a.fields["T__adj"].astype(np.float64)
+    assert float(np.abs(got - want).max()) <= 1e-4 * float(np.abs(want).max())
