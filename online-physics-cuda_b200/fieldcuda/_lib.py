@@ -87,6 +87,10 @@ class fe_field_info(ctypes.Structure):
 
 
 FE_RANGE, FE_NOT_FINITE, FE_CONSERVATION, FE_SUBSTEP_CAP = 0, 1, 2, 3
+class fe_batch_desc(_c.Structure):
+    _fields_ = [("nx", _c.c_int), ("ny", _c.c_int), ("nz", _c.c_int), ("h", _c.c_double)]
+
+
 FE_STEP_IGNORE_MAX_DT = 1
 FE_ADI_DOUGLAS, FE_ADI_HV = 0, 1
 
@@ -154,6 +158,15 @@ SIGNATURES = {
     "fe_law_digest": (_i, [_p, _c.POINTER(_c.c_uint64)]),
     "fe_law_stream": (_i, [_p, _c.POINTER(_p)]),
     "fe_law_time_gather": (_i, [_p, _i, _i, _c.POINTER(_c.c_float)]),
+    "fe_batch_create": (_i, [_cs, _c.POINTER(fe_batch_desc), _i, _c.POINTER(_p)]),
+    "fe_batch_destroy": (None, [_p]),
+    "fe_batch_info": (_i, [_p, _c.POINTER(_i), _c.POINTER(_i)]),
+    "fe_batch_law": (_i, [_p, _i, _c.POINTER(_p), _c.POINTER(_i)]),
+    "fe_batch_set_param": (_i, [_p, _i, _d]),
+    "fe_batch_upload": (_i, [_p, _i, _i, _p]),
+    "fe_batch_fetch": (_i, [_p, _i, _i, _p]),
+    "fe_batch_step": (_i, [_p, _d, _i, _c.POINTER(_i)]),
+    "fe_batch_violation": (_i, [_p, _i, _c.POINTER(_i), _c.POINTER(fe_violation)]),
     "fe_vjp_create": (_i, [_cs, _cs, _i, _i, _i, _d, _c.POINTER(_p)]),
     "fe_vjp_destroy": (None, [_p]),
     "fe_vjp_laws": (_i, [_p, _c.POINTER(_p), _c.POINTER(_p)]),
