@@ -388,6 +388,58 @@ def multifield_section(n, steps, warmup, stream_sync):
             "violations": len(broken)}
 
 
+def nets_section(stream_sync):
+    """The net ops (tests/laws/nets_mlp.law, nets_flux.law, nets_ldiffuse.law) on 128 x 128 x 64 cells, random state:
+    median step time with fp32 nets (per cell on the CUDA cores) and with the nets declared half (tcgen05 stage
+    kernels, BF16 operands, FP32 accumulation), and the half step's worst difference from the fp32 one as a fraction of
+    what the step moved (the reference's gate for its tensor-core nets: 0.03)."""
+    import numpy as np
+    import torch
+    from fieldcuda.solver import Solver
+    here = os.getcwd()
+    os.chdir(ROOT)  # the laws' weight files are repository paths
+    out = {}
+    try:
+        n, nz, dt = 128, 64, 0.02
+        for law in ("nets_mlp.law", "nets_flux.law", "nets_ldiffuse.law"):
+            text = open(os.path.join("tests", "laws", law)).read()
+            row, after = {}, {}
+            for form, t in (("fp32", text), ("half", text.replace(" file ", " half file "))):
+                rng = np.random.default_rng(5)
+                T0 = (290 + 600 * rng.random((nz, n, n))).astype(np.float32)
+                s = Solver(t, n, n, nz, 0.5, law)
+                s.set_field("T", T0)
+                if "fuel" in s.field_names:
+                    s.set_field("fuel", rng.random((nz, n, n)).astype(np.float32))
+                s.step(dt)
+                after[form] = s.values("T").astype(np.float64)
+                s.set_deferred(True)
+                for _ in range(3):
+                    s.step(dt)
+                st = torch.cuda.ExternalStream(s.stream)
+                times = []
+                for _ in range(10):
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    stream_sync()
+                    e0.record(st)
+                    s.step(dt)
+                    e1.record(st)
+                    st.synchronize()
+                    times.append(e0.elapsed_time(e1))
+                s.sync()
+                row[form + "_ms_per_step"] = statistics.median(times)
+                row[form + "_violations"] = len(s.violations())
+                s.close()
+                if form == "fp32":
+                    moved = float(np.abs(after["fp32"] - T0).max())
+            row["speedup"] = row["fp32_ms_per_step"] / row["half_ms_per_step"]
+            row["half_worst_over_moved"] = float(np.abs(after["half"] - after["fp32"]).max()) / max(moved, 1e-30)
+            out[law] = row
+    finally:
+        os.chdir(here)
+    return {"cells": n * n * nz, "dt": dt, "laws": out}
+
+
 HESTON_DOUGLAS_LAW = os.path.join(ROOT, "tests", "laws", "heston_douglas.law")
 HESTON_CALIB = os.path.join(ROOT, "tests", "golden", "heston", "calib_512.npz")
 
@@ -654,6 +706,9 @@ def run_ours(args, world, rank, local):
     learned = None
     if not args.no_learned:
         learned = fhn_learned_section()
+    nets = None
+    if not args.no_nets:
+        nets = nets_section(torch.cuda.synchronize)
 
     if rank != 0:
         return
@@ -683,6 +738,7 @@ def run_ours(args, world, rank, local):
         "multifield_256": multifield,
         "adjoint_calibration": calibration,
         "fhn_learned": learned,
+        "nets_half": nets,
     }))
 
 
@@ -774,6 +830,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-heston", action="store_true", help="skip the batched Heston ADI section")
     ap.add_argument("--no-multifield", action="store_true", help="skip the 43-term multi-field law section")
+    ap.add_argument("--no-nets", action="store_true", help="skip the net ops section (fp32 and tensor-core nets)")
     ap.add_argument("--no-calibration", action="store_true", help="skip the adjoint calibration section")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-correction section")
     ap.add_argument("--profile-case", default="", help="run one small case for ncu (heat, heston, corrector, multifield, nets) and exit")

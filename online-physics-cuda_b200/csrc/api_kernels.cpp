@@ -222,8 +222,9 @@ int fe_heat7_step(const float* T_dev, float* out_dev, int nx, int ny, int nz, fl
 
 int fe_copy_f32(const float* src_dev, float* dst_dev, size_t n, void* stream)
 {
-    if (src_dev == nullptr || dst_dev == nullptr || (n & 3) != 0) {
-        return fail(FE_EINVAL, "fe_copy_f32: bad buffers or size (a multiple of 4 floats)");
+    if (src_dev == nullptr || dst_dev == nullptr || (n & 3) != 0 || (reinterpret_cast<std::uintptr_t>(src_dev) & 15u) != 0 ||
+        (reinterpret_cast<std::uintptr_t>(dst_dev) & 15u) != 0) {
+        return fail(FE_EINVAL, "fe_copy_f32: bad buffers or size (16-byte aligned buffers, a multiple of 4 floats)");
     }
     std::string why;
     if (!device_ready(why)) {

@@ -13,16 +13,26 @@ namespace fe {
 __global__ void __launch_bounds__(256) totals_f32(const float* __restrict__ v, size_t n, FeCheck* rec, double* partials, unsigned* count)
 {
     __shared__ double scratch[4 * 8];
-    // Block b sums cells [b0, b1): a whole number of float4s (the buffer is 256-byte aligned), the last block the tail.
-    const size_t per = ((n + gridDim.x - 1) / gridDim.x + 3) / 4 * 4;
-    const size_t b0 = min(n, per * blockIdx.x);
-    const size_t b1 = min(n, b0 + per);
-    const float4* v4 = reinterpret_cast<const float4*>(v);
+    // `v` may start inside a 16-byte word (a slab's owned planes start at plane * z0 cells): the cells up to the first
+    // 16-byte boundary are block 0's head, the rest is read as float4s from an aligned pointer.
+    const size_t head = min(n, static_cast<size_t>(((16u - (reinterpret_cast<size_t>(v) & 15u)) & 15u) / 4u));
+    const float* w = v + head;
+    const size_t m = n - head;
+    // Block b sums cells [b0, b1) of w: a whole number of float4s, the last non-empty block the tail.
+    const size_t per = ((m + gridDim.x - 1) / gridDim.x + 3) / 4 * 4;
+    const size_t b0 = min(m, per * blockIdx.x);
+    const size_t b1 = min(m, b0 + per);
+    const float4* w4 = reinterpret_cast<const float4*>(w);
     FeAcc acc;
     fe_acc_init(acc);
+    if (blockIdx.x == 0 && threadIdx.x < head) {
+        const double x = static_cast<double>(v[threadIdx.x]);
+        acc.before += x;
+        acc.before_abs += fabs(x);
+    }
 #pragma unroll 4
     for (size_t i = b0 / 4 + threadIdx.x; i < b1 / 4; i += blockDim.x) {
-        const float4 x = __ldg(v4 + i);
+        const float4 x = __ldg(w4 + i);
         acc.before += static_cast<double>(x.x);
         acc.before += static_cast<double>(x.y);
         acc.before += static_cast<double>(x.z);
@@ -32,8 +42,9 @@ __global__ void __launch_bounds__(256) totals_f32(const float* __restrict__ v, s
         acc.before_abs += fabs(static_cast<double>(x.z));
         acc.before_abs += fabs(static_cast<double>(x.w));
     }
-    for (size_t i = b1 / 4 * 4 + threadIdx.x; i < b1; i += blockDim.x) {
-        const double x = static_cast<double>(v[i]);
+    // The tail past the last float4 belongs to the block whose slice holds it (empty slices at the end hold nothing).
+    for (size_t i = max(b0, b1 / 4 * 4) + threadIdx.x; i < b1; i += blockDim.x) {
+        const double x = static_cast<double>(w[i]);
         acc.before += x;
         acc.before_abs += fabs(x);
     }

@@ -96,3 +96,26 @@ def test_half_step_is_deterministic(cuda, monkeypatch):
     assert a.digest() == b.digest()
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (1, 2, 3), (3, 5, 7), (2, 3, 130), (2, 1, 129)], ids=str)
+def test_half_nets_on_ragged_lattices(cuda, shape, monkeypatch):
+    """Lattices smaller than one 128-cell tile, partial last tiles and flat axes (closed faces): the tensor-core stage
+    against the fp32 one, the same gate."""
+    monkeypatch.chdir(ROOT)
+    rng = np.random.default_rng(sum(shape))
+    for law in ("nets_mlp.law", "nets_flux.law", "nets_ldiffuse.law"):
+        text = open(os.path.join(ROOT, "tests", "laws", law)).read()
+        meta = {"shape": list(shape), "h": 0.5, "law": law, "dt": 0.02}
+        init = {"T": (290 + 600 * rng.random(shape)).astype(np.float32)}
+        if "fuel" in text:
+            init["fuel"] = rng.random(shape).astype(np.float32)
+        a, b = solve(half(text), meta, init, 1), solve(text, meta, init, 1)
+        before = init["T"].astype(np.float64)
+        want = b.values("T").astype(np.float64)
+        moved = float(np.abs(want - before).max())
+        worst = float(np.abs(a.values("T").astype(np.float64) - want).max())
+        assert worst <= 0.03 * moved + 1e-3, (law, worst, moved)
+        assert a.violations() == []
+        a.close()
+        b.close()

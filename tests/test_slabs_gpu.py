@@ -48,6 +48,32 @@ def test_heat_slabs_match_the_whole_lattice_bit_for_bit(cuda, size, nx):
     g.close()
 
 
+def test_slabs_whose_planes_are_not_whole_float4s(cuda):
+    """A 5 x 7 plane (35 cells): a slab's owned planes start inside a 16-byte word, and the lattice's cell count is not
+    a multiple of 4. The totals before the first step (a fixed-grid float4 reduction) must count every owned cell once:
+    no conservation break on the slabs or on the whole lattice, and the same bits."""
+    from fieldcuda.slabs import SlabGroup
+    from fieldcuda.solver import Solver
+    shape = (30, 7, 5)
+    h = 1.0 / 32
+    T0 = np.random.default_rng(9).uniform(0, 1, shape).astype(np.float32)
+    dt = 0.4 * h * h / 6
+    s = Solver(HEAT, 5, 7, 30, h)
+    s.set_field("T", T0)
+    for _ in range(4):
+        s.step(dt)
+        assert s.violations() == []
+    want = s.values("T")
+    s.close()
+    g = SlabGroup(HEAT, 5, 7, 30, h, 3)
+    g.set_field("T", T0)
+    for _ in range(4):
+        g.step(dt)
+    assert g.sync() == []
+    assert np.array_equal(g.values("T").view(np.uint32), want.view(np.uint32))
+    g.close()
+
+
 def test_a_leak_is_judged_over_the_slabs_with_the_whole_lattices_totals(cuda):
     from fieldcuda.slabs import SlabGroup
     from fieldcuda.solver import Solver
