@@ -30,7 +30,10 @@ struct fe_vjp {
     std::vector<int> statics, statics_in_adj;
     int steps = 0, every = 1;
     double dt = 0.0;
-    std::vector<float*> checkpoints; // per checkpoint: the state fields, one after the other
+    std::vector<float*> checkpoints; // per checkpoint: the state fields, one after the other (kept across forwards)
+    std::size_t checkpoint_bytes = 0;
+    std::size_t used = 0;            // checkpoints the last forward filled
+    int seen = 0;                    // violations the primal held after the last forward (deferred judging keeps them)
     float* segment = nullptr;        // every x state fields: a segment's recomputed states
     std::size_t segment_states = 0;
 
@@ -45,6 +48,8 @@ struct fe_vjp {
     {
         for (float* p : checkpoints) cudaFree(p);
         checkpoints.clear();
+        checkpoint_bytes = 0;
+        used = 0;
         if (segment != nullptr) cudaFree(segment);
         segment = nullptr;
         segment_states = 0;
@@ -169,21 +174,25 @@ int fe_vjp_forward(fe_vjp* v, double dt, int steps, int every)
 {
     if (v == nullptr) return fe::fail(FE_EINVAL, "fe_vjp_forward: null handle");
     if (steps < 1 || !(dt > 0.0)) return fe::fail(FE_EINVAL, "fe_vjp_forward: steps >= 1 and dt > 0");
-    v->release();
     v->steps = steps;
     v->dt = dt;
     v->every = every > 0 ? every : std::max(1, static_cast<int>(std::ceil(std::sqrt(static_cast<double>(steps)))));
-    const std::size_t bytes = v->cells * v->state.size() * sizeof(float);
-    const int count = (steps + v->every - 1) / v->every;
-    for (int c = 0; c < count; ++c) {
+    const std::size_t bytes = std::max<std::size_t>(v->cells * v->state.size() * sizeof(float), 4);
+    const std::size_t count = static_cast<std::size_t>((steps + v->every - 1) / v->every);
+    // The checkpoint buffers of the last forward serve this one when they fit (a calibration's repeated forwards
+    // allocate once: cudaFree waits for the whole device).
+    if (v->checkpoint_bytes != bytes) v->release();
+    while (v->checkpoints.size() < count) {
         float* p = nullptr;
-        const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), std::max<std::size_t>(bytes, 4));
+        const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), bytes);
         if (e != cudaSuccess) {
             v->release();
             return cuda_fail(e, "cudaMalloc (checkpoint)");
         }
         v->checkpoints.push_back(p);
+        v->checkpoint_bytes = bytes;
     }
+    v->used = 0;
     fe_step_info info{};
     for (int s = 0; s < steps; ++s) {
         int rc = FE_OK;
@@ -196,18 +205,21 @@ int fe_vjp_forward(fe_vjp* v, double dt, int steps, int every)
     }
     int rc = fe_law_sync(v->primal, &info);
     if (rc != FE_OK) return rc;
-    if (info.violations > 0) {
+    const int before = v->seen;
+    v->seen = info.violations;
+    if (info.violations > before) {
         fe_violation bad{};
-        fe_law_violation(v->primal, 0, &bad);
+        fe_law_violation(v->primal, before, &bad);
         return fe::fail(FE_ELAW, std::string("the forward broke a contract: ") + bad.detail);
     }
+    v->used = count;
     return fe::ok();
 }
 
 int fe_vjp_backward(fe_vjp* v)
 {
     if (v == nullptr) return fe::fail(FE_EINVAL, "fe_vjp_backward: null handle");
-    if (v->checkpoints.empty()) return fe::fail(FE_EINVAL, "fe_vjp_backward: no forward to go back over");
+    if (v->used == 0) return fe::fail(FE_EINVAL, "fe_vjp_backward: no forward to go back over");
     const std::size_t per = v->cells * v->state.size();
     const std::size_t want = static_cast<std::size_t>(std::max(v->every, 1)) * std::max<std::size_t>(per, 1);
     if (v->segment_states < want) {
@@ -224,7 +236,7 @@ int fe_vjp_backward(fe_vjp* v)
         if ((rc = fe_law_upload_device(v->adj, v->statics_in_adj[k], v->segment)) != FE_OK) return rc;
     }
     fe_step_info info{};
-    for (int seg = static_cast<int>(v->checkpoints.size()) - 1; seg >= 0; --seg) {
+    for (int seg = static_cast<int>(v->used) - 1; seg >= 0; --seg) {
         const int start = seg * v->every;
         const int end = std::min(v->steps, start + v->every);
         if ((rc = restore_state(v, v->checkpoints[static_cast<std::size_t>(seg)])) != FE_OK) return rc;
