@@ -748,6 +748,8 @@ def profile_case(name):
     heston      36 options on 512 x 256, 16 Douglas steps, split (16, 4, 512): the cluster kernel;
     corrector   3 training steps, one gradient and one guarded apply on 256 x 32 x 32 cells: the tcgen05 kernels;
     multifield  the 43-term law on 128^3, 3 steps: its generated passes;
+    calibration the adjoint calibration's lattice (512 options, 256 x 128) over 4 Douglas steps: one loss and gradient
+                (the forward, the checkpointed recompute and the adjoint law's steps);
     nets        the learned-flux and learned-conduction laws (tests/laws/nets_flux.law, nets_ldiffuse.law) on
                 128 x 128 x 64, 3 steps each with fp32 nets, then with the nets declared half: the tcgen05 net stages."""
     import numpy as np
@@ -797,6 +799,17 @@ def profile_case(name):
         s.sync()
         print(json.dumps({"case": name, "violations": len(s.violations())}))
         s.close()
+    elif name == "calibration":
+        from fieldcuda.heston import Calibration, calibration_options
+        z = np.load(HESTON_CALIB)
+        strikes, common, truth = calibration_options(512, int(z["seed"]))
+        cal = Calibration(open(HESTON_DOUGLAS_LAW).read(), strikes, common["maturity"], common["spot"], common["r"], z["targets"],
+                          256, 128, 4)
+        x = [truth["kappa"] * 1.2, truth["theta"] * 0.9, truth["sigma"] * 1.1, truth["rho"] * 0.9, truth["v0"] * 1.1]
+        loss, grad = cal.loss_and_grad(x)
+        torch.cuda.synchronize()
+        cal.close()
+        print(json.dumps({"case": name, "loss": loss, "grad": [float(g) for g in grad]}))
     elif name == "nets":
         from fieldcuda.solver import Solver
         os.chdir(ROOT)  # the laws' weight files are repository paths

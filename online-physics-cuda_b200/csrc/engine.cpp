@@ -16,6 +16,7 @@ using law::Op;
 
 constexpr int kRing = 64;           // steps of contract records a deferred run may keep on the card
 constexpr int kMaxSubsteps = 4096;  // Solver::kMaxSubsteps (src/field/Solver.hpp:129)
+static_assert(sizeof(FePassArgs) <= 4096, "a generated pass takes its arguments as one kernel parameter of at most 4 KB");
 
 double times(double a, double b)
 {
