@@ -236,18 +236,21 @@ int fe_law_time_gather(fe_law* law, int term, int launches, float* ms);
  * bench/pdebench.py:71-92). fe_batch_create takes n instances of any extents and h. Instances of equal (nx, ny, h) share
  * one lattice, stacked along z in order, when the law couples nothing along z (no value read across planes, no
  * lattice-wide reduction, distance or poisson, no solve along z, no `rim`); otherwise every instance is a lattice of
- * its own (fe_batch_info: how many, and whether stacked). Each lattice is a law handle with its own stream
- * (fe_batch_law: an instance's handle and first plane, for params and profiles); fe_batch_step launches every
- * lattice's step, then judges all their contracts. A stacked lattice's conserved totals are judged over all its
- * instances together, as the reference's z-plane batches are. Violations carry their instance (-1: a conserved total of a
- * lattice holding several), range/NaN cells numbered within the instance. fe_batch_set_param sets a param everywhere;
- * fe_batch_upload / _fetch move one instance's field (nx*ny*nz floats, x fastest) from / to the host. */
+ * its own (fe_batch_info: how many, and whether stacked; fe_batch_plan: the same grouping without a device). Each
+ * lattice is a law handle with its own stream (fe_batch_law: an instance's handle and first plane, for params and
+ * profiles); fe_batch_step launches every lattice's step, then judges all their contracts. A stacked lattice's
+ * conserved totals are judged over all its instances together, as the reference's z-plane batches are. Violations
+ * carry their instance (-1: a conserved total of a lattice holding several), range/NaN cells numbered within the
+ * instance. fe_batch_set_param sets a param everywhere; fe_batch_upload / _fetch move one instance's field
+ * (nx*ny*nz floats, x fastest) from / to the host. */
 typedef struct fe_batch_desc {
     int nx, ny, nz;
     double h;
 } fe_batch_desc;
 typedef struct fe_batch fe_batch;
 int fe_batch_create(const char* law_text, const fe_batch_desc* descs, int n, fe_batch** out);
+/* lattice_of and z0: arrays of n (or NULL) that get each instance's lattice and its first plane there. */
+int fe_batch_plan(const char* law_text, const fe_batch_desc* descs, int n, int* lattices, int* stacked, int* lattice_of, int* z0);
 void fe_batch_destroy(fe_batch* batch);
 int fe_batch_info(const fe_batch* batch, int* lattices, int* stacked);
 int fe_batch_law(fe_batch* batch, int instance, fe_law** law, int* z0);

@@ -71,6 +71,52 @@ bool planes_independent(const char* law_text, int nx, int ny, double h, std::str
     return reach == 0 && !reductions && !z_solves;
 }
 
+// Which lattice each instance goes into (equal nx, ny, h stacked when the planes are independent), the lattices'
+// extents, and each instance's first plane.
+struct Grouping {
+    bool stacked = false;
+    std::vector<fe_batch::Lattice> lattices;
+    std::vector<fe_batch::Where> where;
+};
+
+int group_instances(const char* law_text, const fe_batch_desc* descs, int n, Grouping& g)
+{
+    if (law_text == nullptr || descs == nullptr || n < 1) return fe::fail(FE_EINVAL, "fe_batch: bad argument");
+    for (int i = 0; i < n; ++i) {
+        if (descs[i].nx < 1 || descs[i].ny < 1 || descs[i].nz < 1 || !(descs[i].h > 0.0)) {
+            return fe::fail(FE_EINVAL, "fe_batch: instance " + std::to_string(i) + " has a bad lattice");
+        }
+    }
+    std::string why;
+    g.stacked = planes_independent(law_text, descs[0].nx, descs[0].ny, descs[0].h, why);
+    if (!why.empty()) return fe::fail(FE_ELAW, why);
+    g.where.resize(static_cast<std::size_t>(n));
+    std::map<std::tuple<int, int, double>, int> by_shape;
+    for (int i = 0; i < n; ++i) {
+        const fe_batch_desc& d = descs[i];
+        int at = -1;
+        if (g.stacked) {
+            const auto key = std::make_tuple(d.nx, d.ny, d.h);
+            const auto found = by_shape.find(key);
+            if (found != by_shape.end()) at = found->second;
+            else by_shape.emplace(key, at = static_cast<int>(g.lattices.size()));
+        }
+        if (at < 0 || static_cast<std::size_t>(at) == g.lattices.size()) {
+            at = static_cast<int>(g.lattices.size());
+            fe_batch::Lattice l;
+            l.nx = d.nx;
+            l.ny = d.ny;
+            l.h = d.h;
+            g.lattices.push_back(l);
+        }
+        fe_batch::Lattice& l = g.lattices[static_cast<std::size_t>(at)];
+        g.where[static_cast<std::size_t>(i)] = fe_batch::Where{at, l.nz, d.nz};
+        l.nz += d.nz;
+        l.members.push_back(i);
+    }
+    return fe::ok();
+}
+
 bool instance_ok(const fe_batch* b, int instance)
 {
     return b != nullptr && instance >= 0 && static_cast<std::size_t>(instance) < b->where.size();
@@ -110,47 +156,34 @@ extern "C" {
 
 int fe_batch_create(const char* law_text, const fe_batch_desc* descs, int n, fe_batch** out)
 {
-    if (law_text == nullptr || descs == nullptr || out == nullptr || n < 1) return fe::fail(FE_EINVAL, "fe_batch_create: bad argument");
+    if (out == nullptr) return fe::fail(FE_EINVAL, "fe_batch_create: null argument");
     *out = nullptr;
-    for (int i = 0; i < n; ++i) {
-        if (descs[i].nx < 1 || descs[i].ny < 1 || descs[i].nz < 1 || !(descs[i].h > 0.0)) {
-            return fe::fail(FE_EINVAL, "fe_batch_create: instance " + std::to_string(i) + " has a bad lattice");
-        }
-    }
+    Grouping g;
+    int rc = group_instances(law_text, descs, n, g);
+    if (rc != FE_OK) return rc;
     auto b = std::make_unique<fe_batch>();
-    std::string why;
-    b->stacked = planes_independent(law_text, descs[0].nx, descs[0].ny, descs[0].h, why);
-    if (!why.empty()) return fe::fail(FE_ELAW, why);
-    b->where.resize(static_cast<std::size_t>(n));
-    std::map<std::tuple<int, int, double>, int> by_shape;
-    for (int i = 0; i < n; ++i) {
-        const fe_batch_desc& d = descs[i];
-        int at = -1;
-        if (b->stacked) {
-            const auto key = std::make_tuple(d.nx, d.ny, d.h);
-            const auto found = by_shape.find(key);
-            if (found != by_shape.end()) at = found->second;
-            else by_shape.emplace(key, at = static_cast<int>(b->lattices.size()));
-        }
-        if (at < 0 || static_cast<std::size_t>(at) == b->lattices.size()) {
-            at = static_cast<int>(b->lattices.size());
-            fe_batch::Lattice l;
-            l.nx = d.nx;
-            l.ny = d.ny;
-            l.h = d.h;
-            b->lattices.push_back(l);
-        }
-        fe_batch::Lattice& l = b->lattices[static_cast<std::size_t>(at)];
-        b->where[static_cast<std::size_t>(i)] = fe_batch::Where{at, l.nz, d.nz};
-        l.nz += d.nz;
-        l.members.push_back(i);
-    }
+    b->stacked = g.stacked;
+    b->where = std::move(g.where);
+    b->lattices = std::move(g.lattices);
     for (fe_batch::Lattice& l : b->lattices) {
-        int rc = fe_law_create(law_text, "batch", l.nx, l.ny, l.nz, l.h, &l.law);
-        if (rc != FE_OK) return rc;
+        if ((rc = fe_law_create(law_text, "batch", l.nx, l.ny, l.nz, l.h, &l.law)) != FE_OK) return rc;
         if ((rc = fe_law_set_deferred(l.law, 1)) != FE_OK) return rc;
     }
     *out = b.release();
+    return fe::ok();
+}
+
+int fe_batch_plan(const char* law_text, const fe_batch_desc* descs, int n, int* lattices, int* stacked, int* lattice_of, int* z0)
+{
+    Grouping g;
+    const int rc = group_instances(law_text, descs, n, g);
+    if (rc != FE_OK) return rc;
+    if (lattices != nullptr) *lattices = static_cast<int>(g.lattices.size());
+    if (stacked != nullptr) *stacked = g.stacked ? 1 : 0;
+    for (int i = 0; i < n; ++i) {
+        if (lattice_of != nullptr) lattice_of[i] = g.where[static_cast<std::size_t>(i)].lattice;
+        if (z0 != nullptr) z0[i] = g.where[static_cast<std::size_t>(i)].z0;
+    }
     return fe::ok();
 }
 

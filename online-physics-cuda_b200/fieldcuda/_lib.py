@@ -160,6 +160,7 @@ SIGNATURES = {
     "fe_law_time_gather": (_i, [_p, _i, _i, _c.POINTER(_c.c_float)]),
     "fe_batch_create": (_i, [_cs, _c.POINTER(fe_batch_desc), _i, _c.POINTER(_p)]),
     "fe_batch_destroy": (None, [_p]),
+    "fe_batch_plan": (_i, [_cs, _c.POINTER(fe_batch_desc), _i, _c.POINTER(_i), _c.POINTER(_i), _p, _p]),
     "fe_batch_info": (_i, [_p, _c.POINTER(_i), _c.POINTER(_i)]),
     "fe_batch_law": (_i, [_p, _i, _c.POINTER(_p), _c.POINTER(_i)]),
     "fe_batch_set_param": (_i, [_p, _i, _d]),
