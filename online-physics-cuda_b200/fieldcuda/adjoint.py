@@ -53,6 +53,9 @@ class LawVJP:
 
     def close(self):
         if getattr(self, "_v", None) is not None and self._v.value:
+            for view in (getattr(self, "primal", None), getattr(self, "adj", None)):
+                if view is not None:
+                    view.close()  # a borrowed view: forgets the handle, which fe_vjp_destroy frees
             self._lib.fe_vjp_destroy(self._v)
             self._v = ctypes.c_void_p()
 

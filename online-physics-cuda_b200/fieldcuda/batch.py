@@ -38,6 +38,8 @@ class LawBatch:
 
     def close(self):
         if getattr(self, "_b", None) is not None and self._b.value:
+            if getattr(self, "_names", None) is not None:
+                self._names.close()  # a borrowed view: forgets the handle, which fe_batch_destroy frees
             self._lib.fe_batch_destroy(self._b)
             self._b = ctypes.c_void_p()
 
