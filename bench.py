@@ -745,6 +745,8 @@ def run_ours(args, world, rank, local):
 def profile_case(name):
     """Small cases of the kernels the profiles under profiles/ summarise, for ncu (one GPU; a few launches):
     heat        the heat law on 512^3 (the bench's lattice; inputs larger than L2), 3 steps: the generated gather;
+    heat256     the same law on 256^3 (two 64 MiB fields: still larger than L2 together), 3 steps: the gather's instruction
+                mix (more metrics than the 512^3 case should carry);
     heston      36 options on 512 x 256, 16 Douglas steps, split (16, 4, 512): the cluster kernel;
     corrector   3 training steps, one gradient and one guarded apply on 256 x 32 x 32 cells: the tcgen05 kernels;
     multifield  the 43-term law on 128^3, 3 steps: its generated passes;
@@ -773,10 +775,10 @@ def profile_case(name):
         torch.cuda.synchronize()
         c.close()
         print(json.dumps({"case": name, "loss": loss}))
-    elif name == "heat":
+    elif name in ("heat", "heat256"):
         from fieldcuda.solver import Solver
         from oracle import heat as oh
-        n = 512
+        n = 512 if name == "heat" else 256
         h = 1.0 / n
         s = Solver(HEAT_LAW, n, n, n, h, "heat.law")
         s.set_field("T", oh.gaussian_blobs(n, h, seed=0))
