@@ -1083,6 +1083,7 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
           << ", L = " << layers << ", NMAX = " << nmax << ", KP0 = " << kp[0] << ";\n"
           << "    static constexpr unsigned TCOLS = " << tcols << "u, A_BYTES = " << a_bytes << "u, W_BYTES = " << wbytes << "u, WOFF = " << na.bf16_bytes
           << "u;\n"
+          << "    static constexpr bool ROLL = " << (e * layers > 24 ? "true" : "false") << ";\n"
           << "    static constexpr float OSCALE = " << literal(net.out_scale) << ";\n";
         fn("int", "kp", kp);
         fn("int", "np", np);

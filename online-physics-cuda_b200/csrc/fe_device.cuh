@@ -1104,8 +1104,10 @@ __device__ __forceinline__ void fe_net_pass(const FePassArgs& a, const unsigned 
         typename P::Keep keep;
         P::prepare(c, x, y, z, keep);
         float o = 0.f;
-#pragma unroll
-        for (int ch = 0; ch < P::E; ch += P::EC) {
+        // One chunk of a cell's evaluations through every layer. A deep net's chunks stay one copy of the code (the
+        // unrolled form outgrows the instruction cache: ldiffuse 5-8-8-4, 0.27 -> 0.23 ms a step at 1M cells); a
+        // shallow one's are unrolled, which lets the gathered inputs stay in registers.
+        auto chunk = [&](int ch) {
             // Layer 0's operands: the inputs, shifted and scaled (FP32), then BF16; zeros past the net's inputs.
 #pragma unroll
             for (int ee = 0; ee < P::EC; ++ee) {
@@ -1166,6 +1168,13 @@ __device__ __forceinline__ void fe_net_pass(const FePassArgs& a, const unsigned 
             }
 #pragma unroll
             for (int ee = 0; ee < P::EC; ee += P::PAIR) P::take(keep, ch + ee, yout[ee], yout[ee + P::PAIR - 1], o);
+        };
+        if constexpr (P::ROLL) {
+#pragma unroll 1
+            for (int ch = 0; ch < P::E; ch += P::EC) chunk(ch);
+        } else {
+#pragma unroll
+            for (int ch = 0; ch < P::E; ch += P::EC) chunk(ch);
         }
         if (ok && valid) a.out[0][cell] = P::result(o);
     }
