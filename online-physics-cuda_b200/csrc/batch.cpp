@@ -50,25 +50,27 @@ struct fe_batch {
 
 namespace {
 
-// Whether the law's step on a lattice leaves every z-plane's update to that plane alone.
-bool planes_independent(const char* law_text, int nx, int ny, double h, std::string& why)
+// Whether the law's step on a lattice leaves every z-plane's update to that plane alone (*independent); FE_ELAW when
+// the law does not compile, FE_EUNSUP when this backend cannot run it.
+int planes_independent(const char* law_text, int nx, int ny, double h, bool* independent)
 {
     std::vector<std::string> errors;
     const fe::law::Law law = fe::law::compile({fe::law::Source{"law", law_text}}, errors);
     if (!errors.empty()) {
+        std::string why;
         for (const std::string& e : errors) why += e + "\n";
-        return false;
+        return fe::fail(FE_ELAW, why);
     }
     const fe::ir::Module m = fe::ir::lower(law);
-    for (const fe::ir::Inst& in : m.insts) {
-        if (in.op == fe::law::Op::Rim) return false;
-    }
     fe::gen::Plan plan;
-    if (!fe::gen::generate(m, law, nx, ny, 2, h, plan, why)) return false;
+    std::string why;
+    if (!fe::gen::generate(m, law, nx, ny, 2, h, plan, why)) return fe::fail(FE_EUNSUP, why);
     int reach = 0;
     bool reductions = false, z_solves = false;
     fe::plan_z_reach(plan, reach, reductions, z_solves);
-    return reach == 0 && !reductions && !z_solves;
+    const bool rim = std::any_of(m.insts.begin(), m.insts.end(), [](const fe::ir::Inst& in) { return in.op == fe::law::Op::Rim; });
+    *independent = reach == 0 && !reductions && !z_solves && !rim;
+    return fe::ok();
 }
 
 // Which lattice each instance goes into (equal nx, ny, h stacked when the planes are independent), the lattices'
@@ -87,9 +89,8 @@ int group_instances(const char* law_text, const fe_batch_desc* descs, int n, Gro
             return fe::fail(FE_EINVAL, "fe_batch: instance " + std::to_string(i) + " has a bad lattice");
         }
     }
-    std::string why;
-    g.stacked = planes_independent(law_text, descs[0].nx, descs[0].ny, descs[0].h, why);
-    if (!why.empty()) return fe::fail(FE_ELAW, why);
+    const int rc = planes_independent(law_text, descs[0].nx, descs[0].ny, descs[0].h, &g.stacked);
+    if (rc != FE_OK) return rc;
     g.where.resize(static_cast<std::size_t>(n));
     std::map<std::tuple<int, int, double>, int> by_shape;
     for (int i = 0; i < n; ++i) {

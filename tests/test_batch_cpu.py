@@ -45,3 +45,5 @@ def test_bad_instances_are_refused():
     from fieldcuda import _lib
     with pytest.raises(_lib.FeError, match="bad lattice"):
         plan(text("fhn_rk4.law"), [(4, 4, 0, 0.1)])
+    with pytest.raises(_lib.FeError, match="unknown"):
+        plan("field T init 0\nterm t\n  d T = sprinkle(T)\n", [(4, 4, 1, 0.1)])
