@@ -185,7 +185,7 @@ int fe_law_fetch_device(fe_law* law, int field, float* dev);
 int fe_law_mark_edited(fe_law* law, int field);
 
 /* A lattice split along z over ranks (no counterpart in the reference, whose CudaSolver runs one lattice on one GPU;
- * SURVEY's multi-GPU form of CudaSolver::step). A rank's handle holds its slab plus halo planes copied from its
+ * the z-slab form of CudaSolver::step over several GPUs). A rank's handle holds its slab plus halo planes copied from its
  * neighbours after every step:
  *   fe_law_set_owned_z: contracts (totals, bounds, range, change flag) cover planes [z0, z1) only;
  *   fe_law_mark_halo: the field's halo planes were written by the caller (its bounds are forgotten, the owned totals kept);
