@@ -174,13 +174,15 @@ def scene_fixtures(lawc):
     scene makes (step_0, after refresh_derived) and the state after the steps, for the CLI's parity tests."""
     out_dir = os.path.join(HERE, "scene")
     os.makedirs(out_dir, exist_ok=True)
-    for name, steps, dt in (("ops", 3, 0.05),):
+    # guarded: heat with an untrained learned scheme at twice the stable step, run with --learned: which learned steps
+    # the reference's guard undoes, and the state that leaves.
+    for name, steps, dt, extra in (("ops", 3, 0.05, []), ("guarded", 30, 0.3, ["--learned"])):
         work = tempfile.mkdtemp(prefix="fe_scene_")
         try:
             dump = os.path.join(work, "dump")
             js = os.path.join(work, "t.json")
             subprocess.run([lawc, "--scene", os.path.join("tests", "scenes", name + ".scene"), "--steps", str(steps), "--dt", repr(dt),
-                            "--dump", dump, "--json", js], check=True, capture_output=True, cwd=ROOT,
+                            "--dump", dump, "--json", js] + extra, check=True, capture_output=True, cwd=ROOT,
                            env=dict(os.environ, OMP_NUM_THREADS="4"))
             meta_dump = json.load(open(os.path.join(dump, "step_0", "meta.json")))
             shape = (meta_dump["nz"], meta_dump["ny"], meta_dump["nx"])
@@ -190,7 +192,8 @@ def scene_fixtures(lawc):
                     arrays[f"step{k}_{f}"] = np.fromfile(os.path.join(dump, f"step_{k}", f + ".bin"), np.float32).reshape(shape)
             timing = json.load(open(js))
             meta = dict(scene=name + ".scene", steps=steps, dt=dt, fields=meta_dump["fields"], substeps=timing["substeps"],
-                        violations=timing["violations"], made_by="the reference's lawc --scene (its OpenMP CPU Solver)")
+                        violations=timing["violations"], fallbacks=timing["fallbacks"], flags=extra,
+                        made_by="the reference's lawc --scene (its OpenMP CPU Solver)")
             np.savez_compressed(os.path.join(out_dir, name + ".npz"), meta=json.dumps(meta), **arrays)
             print("scene", name)
         finally:

@@ -29,6 +29,17 @@ def test_scene_ops_make_the_reference_starting_state():
         assert np.array_equal(got[name].view(np.uint32), want.view(np.uint32)), name
 
 
+def test_scene_guarded_makes_the_reference_starting_state():
+    from fieldcuda import lawc
+    from fieldcuda.solver import ir_json
+    meta, z = fixture("guarded")
+    scene = lawc.load_scene(os.path.join(ROOT, "tests", "scenes", "guarded.scene"))
+    law = open(os.path.join(ROOT, scene.laws[0])).read()
+    inits = {f["name"]: f["init"] for f in json.loads(ir_json(law))["fields"]}
+    got = lawc.scene_fields(scene, list(inits), inits)
+    assert np.array_equal(got["T"].view(np.uint32), z["step0_T"].view(np.uint32))
+
+
 def test_noise_is_a_pure_function_of_seed_and_cell():
     from fieldcuda.lawc import cell_noise
     idx = np.arange(1000, dtype=np.uint64)

@@ -86,3 +86,21 @@ def test_vjp_matches_the_oracle_reverse_pass(cuda, tmp_path, monkeypatch):
         a.step(dt)
     want = a.fields["T__adj"].astype(np.float64)
     assert float(np.abs(got - want).max()) <= 1e-4 * float(np.abs(want).max())
+
+
+def test_guarded_scene_matches_the_reference_lawc(cuda, tmp_path, monkeypatch):
+    """lawc --learned on the guarded scene against the reference's lawc --learned (tests/golden/scene/guarded.npz): the
+    guard undoes the same learned steps (the count), and the state they leave agrees to the whole-law gate."""
+    from fieldcuda import lawc
+    z = np.load(os.path.join(ROOT, "tests", "golden", "scene", "guarded.npz"))
+    meta = json.loads(str(z["meta"]))
+    monkeypatch.chdir(ROOT)
+    dump, js = tmp_path / "dump", tmp_path / "g.json"
+    rc = lawc.main(["--scene", "tests/scenes/guarded.scene", "--steps", str(meta["steps"]), "--dt", repr(meta["dt"]), "--learned",
+                    "--dump", str(dump), "--every", str(meta["steps"]), "--json", str(js)])
+    assert rc == 0
+    out = json.loads(js.read_text())
+    assert out["fallbacks"] == meta["fallbacks"] and out["violations"] == meta["violations"] == 0
+    got = np.fromfile(dump / f"step_{meta['steps']}" / "T.bin", np.float32).reshape(z["step30_T"].shape).astype(np.float64)
+    want = z["step30_T"].astype(np.float64)
+    assert float(np.abs(got - want).max()) <= 1e-4 * float(np.abs(want).max())
