@@ -200,6 +200,33 @@ def scene_fixtures(lawc):
             shutil.rmtree(work, ignore_errors=True)
 
 
+def vjp_fixture(lawc):
+    """lawc --vjp on tests/scenes/heat_vjp.scene: a seeded cotangent of the state after 12 steps stepped back by the
+    reference's own reverse-mode driver (every state kept), and the cotangents of the start it gives (T and the param
+    D), for pinning the adjoint law and the oracle's reverse pass."""
+    out_dir = os.path.join(HERE, "scene")
+    steps, h = 12, 0.05
+    dt = 0.4 * h * h / 6.0 * 0.9
+    shape = (6, 20, 24)
+    seed = np.random.default_rng(11).normal(size=shape).astype(np.float32)
+    work = tempfile.mkdtemp(prefix="fe_vjp_")
+    try:
+        seed_dir, dump = os.path.join(work, "seed"), os.path.join(work, "out")
+        os.makedirs(seed_dir)
+        seed.tofile(os.path.join(seed_dir, "T__adj.bin"))
+        with open(os.path.join(seed_dir, "meta.json"), "w") as f:
+            json.dump({"nx": shape[2], "ny": shape[1], "nz": shape[0], "h": h, "fields": ["T__adj"]}, f)
+        subprocess.run([lawc, "--scene", os.path.join("tests", "scenes", "heat_vjp.scene"), "--steps", str(steps), "--dt", repr(dt),
+                        "--vjp", seed_dir, "--dump", dump], check=True, capture_output=True, cwd=ROOT,
+                       env=dict(os.environ, OMP_NUM_THREADS="4"))
+        arrays = {f: np.fromfile(os.path.join(dump, "adjoint", f + ".bin"), np.float32).reshape(shape) for f in ("T__adj", "D__adj")}
+        meta = dict(scene="heat_vjp.scene", steps=steps, dt=dt, made_by="the reference's lawc --vjp (its CPU Solver)")
+        np.savez_compressed(os.path.join(out_dir, "heat_vjp.npz"), meta=json.dumps(meta), seed=seed, **arrays)
+        print("vjp heat_vjp")
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--lawc", default=os.path.join(ROOT, "oracle", "_ref", "lawc"))
@@ -209,6 +236,7 @@ def main():
         sys.exit(f"no reference solver at {args.lawc}: build it with `make -C oracle ref`")
     ir_fixtures(args.lawc)
     scene_fixtures(args.lawc)
+    vjp_fixture(args.lawc)
     for case in cases():
         if args.only and case["name"] not in args.only.split(","):
             continue

@@ -51,3 +51,35 @@ def test_heat_restatement_matches_the_law_oracle():
     s.fields["T"] = T0.copy()
     s.step(dt)
     assert np.array_equal(s.fields["T"].view(np.uint32), oh.cpu_step(T0, 1.0, h, dt).view(np.uint32))
+
+
+def test_reverse_pass_reproduces_the_reference_vjp():
+    """The adjoint law this backend builds (fe_law_adjoint), run by the oracle back over every kept state, against the
+    reference's own lawc --vjp on the same scene and seed (tests/golden/scene/heat_vjp.npz): bit for bit, for the
+    state's cotangent and the param's."""
+    from fieldcuda import _lib, lawc
+    from fieldcuda.adjoint import adjoint_law
+    from oracle import law_cpu
+    z = np.load(os.path.join(ROOT, "tests", "golden", "scene", "heat_vjp.npz"))
+    meta = json.loads(str(z["meta"]))
+    scene = lawc.load_scene(os.path.join(ROOT, "tests", "scenes", meta["scene"]))
+    nx, ny, nz, h = scene.grid
+    law = open(os.path.join(ROOT, "tests", "laws", "heat.law")).read()
+
+    def solver(text, fields):
+        s = law_cpu.Solver(law_cpu.Law(json.loads(_lib.text_call("fe_law_ir_json", text.encode()))), (nz, ny, nx), h)
+        for k, v in fields.items():
+            s.fields[k] = np.asarray(v, law_cpu.F32).copy()
+        return s
+    start = lawc.scene_fields(scene, ["T"], {"T": 0.0})
+    o = solver(law, start)
+    states = []
+    for _ in range(meta["steps"]):
+        states.append(o.fields["T"].copy())
+        o.step(meta["dt"])
+    a = solver(adjoint_law(law), dict(start, T__adj=z["seed"]))
+    for s in range(meta["steps"] - 1, -1, -1):
+        a.fields["T"] = states[s]
+        a.step(meta["dt"])
+    for name in ("T__adj", "D__adj"):
+        assert np.array_equal(a.fields[name].view(np.uint32), z[name].view(np.uint32)), name
