@@ -83,10 +83,16 @@ int fe_copy_f32(const float* src_dev, float* dst_dev, size_t n, void* stream);
  * cudaMalloc's synchronisation in their loop). It has no counterpart in the reference. The contract pass's per-block
  * partial sums live in a fixed array in the library's device memory (every GPU that loads the library holds it, about
  * 256 KiB, until exit), which limits a pass to 8192 thread blocks: larger lattices are refused with FE_EINVAL (raise
- * zchunk). The caller passes the field buffers and, with `check`, a device fe_check `record_dev` that the call clears
- * and fills (a kernel error word lands in record_dev->pad[0]). The array is shared by every call; each call clears
- * what must start at zero, and calls that overlap on the GPU race on it. The first call on a device looks up the
- * array's device address (once per device, with that device current). Nothing here calls cudaMalloc or cudaFree. */
+ * zchunk). The caller passes the field buffers and a device fe_check `record_dev`, which the call clears and the pass
+ * fills: needed with `check` (the contracts) and with a TMA variant (variant >= 0) even without `check`, since a
+ * bounded wait that gives up raises the kernel's error word in record_dev->pad[0] (bit 1: a wait gave up; 0: none),
+ * which the caller reads after the stream has run; optional for the plain kernel without `check`. The array is shared by every
+ * call; each call clears what must start at zero, and calls that overlap on the GPU (several streams or host threads)
+ * race on it: serialise them on one stream. The first call on a device looks up the array's device address (once per
+ * device, with that device current); that first call may load the library's device code and with it create the
+ * array, so make one call (for example on a one-cell lattice) before a region that may not allocate and before any
+ * stream capture. The address is kept for the device's primary context: after cudaDeviceReset, or from another
+ * context, it is stale. Nothing here calls cudaMalloc or cudaFree. */
 int fe_heat7_step_noalloc(const float* T_dev, float* out_dev, int nx, int ny, int nz, float k, float h, float dt, float lo,
     float hi, int variant, int zchunk, int check, fe_check* record_dev, void* stream);
 
@@ -192,8 +198,9 @@ int fe_law_mark_edited(fe_law* law, int field);
  *   fe_law_set_external_conservation: checked steps log each conserves group's totals (fe_law_take_totals, which hands
  *     over and clears the log, at most `max`, *n the count) instead of judging them: the caller sums over ranks;
  *   fe_law_plan_z_reach: for law text on a lattice (planned, not compiled): planes along z one step reads beyond a cell
- *     (*reach, summed over the step's passes) and flags: 1 the law reduces over the lattice, 2 it solves along z
- *     (neither splits into slabs). */
+ *     (*reach, summed over the step's passes; a term with learned equations counts the larger of its learned and
+ *     classical passes) and flags: 1 the law reduces over the lattice, 2 it solves along z (neither splits into slabs;
+ *     learned equations included, whether or not fe_law_set_learned turns them on later). */
 int fe_law_set_owned_z(fe_law* law, int z0, int z1);
 int fe_law_mark_halo(fe_law* law, int field);
 int fe_law_set_external_conservation(fe_law* law, int on);

@@ -480,19 +480,29 @@ void plan_z_reach(const gen::Plan& plan, int& reach, bool& reductions, bool& z_s
     reach = 0;
     reductions = false;
     z_solves = false;
-    auto count = [&](const gen::Launch& L) {
-        if (L.kind == gen::Launch::Pass || L.kind == gen::Launch::Net) reach += L.rz;
-        if (L.kind == gen::Launch::Reduce || L.kind == gen::Launch::Distance || L.kind == gen::Launch::Poisson) reductions = true;
-        if (L.kind == gen::Launch::TridiagYZ && L.axis == 2) z_solves = true;
+    // The planes along z one program reads beyond a cell, summed over its launches in order.
+    auto program_reach = [&](const gen::ProgramPlan& pp) {
+        int r = 0;
+        if (pp.empty) return r;
+        auto count = [&](const gen::Launch& L) {
+            if (L.kind == gen::Launch::Pass || L.kind == gen::Launch::Net) r += L.rz;
+            if (L.kind == gen::Launch::Reduce || L.kind == gen::Launch::Distance || L.kind == gen::Launch::Poisson) reductions = true;
+            if (L.kind == gen::Launch::TridiagYZ && L.axis == 2) z_solves = true;
+        };
+        for (const gen::Launch& L : pp.stages) count(L);
+        for (const gen::Launch& L : pp.limit) count(L);
+        count(pp.gather);
+        return r;
     };
-    for (const auto* progs : {&plan.terms, &plan.derives}) {
-        for (const gen::ProgramPlan& pp : *progs) {
-            if (pp.empty) continue;
-            for (const gen::Launch& L : pp.stages) count(L);
-            for (const gen::Launch& L : pp.limit) count(L);
-            count(pp.gather);
-        }
+    // A term runs either its learned equations (kept) or its classical ones (the learned step undone, or learned
+    // schemes off), never both on the same state: its reach is the larger of the two. The learned programs are
+    // scanned even while learned schemes are off, since a caller may turn them on after planning.
+    for (std::size_t t = 0; t < plan.terms.size(); ++t) {
+        int r = program_reach(plan.terms[t]);
+        if (t < plan.learned.size()) r = std::max(r, program_reach(plan.learned[t]));
+        reach += r;
     }
+    for (const gen::ProgramPlan& pp : plan.derives) reach += program_reach(pp);
 }
 
 void Engine::mark_edited(int field)

@@ -47,8 +47,9 @@ struct GroupTotals {
     double before = 0.0, after = 0.0, scale = 0.0;
 };
 
-// How many planes along z one step of a planned law reads beyond a cell (the sum over its passes, in order), and whether
-// it reduces over the lattice or solves along z (neither splits into z-slabs).
+// How many planes along z one step of a planned law reads beyond a cell (the sum over its passes, in order; a term with
+// learned equations counts the larger of its learned and classical programs), and whether it reduces over the lattice
+// or solves along z (neither splits into z-slabs), its learned programs included.
 void plan_z_reach(const gen::Plan& plan, int& reach, bool& reductions, bool& z_solves);
 
 struct TermProfile {

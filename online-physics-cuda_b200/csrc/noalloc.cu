@@ -7,9 +7,14 @@
 // scratch in a fixed array in the library's own device memory instead, sized for at most kMaxBlocks thread blocks.
 // Every GPU that loads the library holds the array (about 256 KiB) until the process exits.
 //
-// The array is shared by every call: each call clears what must start at zero (the block counter and the error word)
-// before its kernel, and calls whose kernels overlap on the GPU (several streams, several host threads) race on it.
-// Serialise them on one stream.
+// The array is shared by every call: each call clears what must start at zero (the block counter, and the caller's
+// record with its error word) before its kernel, and calls whose kernels overlap on the GPU (several streams, several
+// host threads) race on it. Serialise them on one stream.
+//
+// The first call on a device looks up the array's device address. That lookup may be what loads the library's device
+// code on that device, and so what creates the array: a caller that may not allocate inside some region (or captures
+// a stream) makes one call before it. The address is kept per device for the primary context; cudaDeviceReset makes
+// it stale.
 #include "../../include/fe.h"
 
 #include "api_common.hpp"
@@ -74,6 +79,11 @@ extern "C" int fe_heat7_step_noalloc(const float* T_dev, float* out_dev, int nx,
     if (check && record_dev == nullptr) {
         return fail(FE_EINVAL, "fe_heat7_step_noalloc: contracts need a record (a device fe_check)");
     }
+    // A TMA variant's bounded waits report a wait that gave up through an error word, which must reach the caller:
+    // it lands in the record, so these variants need one even without contracts (fe_heat7_step asks a workspace).
+    if (variant >= 0 && record_dev == nullptr) {
+        return fail(FE_EINVAL, "fe_heat7_step_noalloc: the TMA variants need a record (a device fe_check, for their error word)");
+    }
     const int blocks = variant < 0 ? heat7_plain_blocks(nx, ny, nz, zchunk) : heat7_tma_blocks(variant, nx, ny, nz, zchunk);
     if (blocks > kMaxBlocks) {
         return fail(FE_EINVAL, "fe_heat7_step_noalloc: this lattice needs " + std::to_string(blocks) + " thread blocks; the fixed scratch holds " +
@@ -84,9 +94,11 @@ extern "C" int fe_heat7_step_noalloc(const float* T_dev, float* out_dev, int nx,
     void* scratch = nullptr;
     if (!scratch_address(&scratch, why)) return fail(FE_ECUDA, why);
     const cudaStream_t s = static_cast<cudaStream_t>(stream);
-    // The previous call's counter and error word are still in the array: clear them, and the caller's record.
+    // The previous call's block counter is still in the array: clear it, and the caller's record (its error word too).
     if (!cuda_ok(cudaMemsetAsync(scratch, 0, kHeader, s), "clear scratch", why)) return fail(FE_ECUDA, why);
-    if (check && !cuda_ok(cudaMemsetAsync(record_dev, 0, sizeof(fe_check), s), "clear record", why)) return fail(FE_ECUDA, why);
+    if (record_dev != nullptr && !cuda_ok(cudaMemsetAsync(record_dev, 0, sizeof(fe_check), s), "clear record", why)) {
+        return fail(FE_ECUDA, why);
+    }
     unsigned char* base = static_cast<unsigned char*>(scratch);
     HeatArgs a{};
     a.out = out_dev;
@@ -103,8 +115,9 @@ extern "C" int fe_heat7_step_noalloc(const float* T_dev, float* out_dev, int nx,
     a.totals_before = (check & FE_HEAT7_BEFORE) ? 1 : 0;
     a.totals_after = (check & FE_HEAT7_AFTER) ? 1 : 0;
     a.rec = check ? reinterpret_cast<FeCheck*>(record_dev) : nullptr;
-    // A kernel's error word lands in the caller's record (pad[0]) when there is one, else in the scratch.
-    a.err = check ? &record_dev->pad[0] : reinterpret_cast<unsigned*>(base);
+    // A kernel's error word lands in the caller's record (pad[0]). Without one (the plain kernel without contracts,
+    // which has no waits) there is none, as with fe_heat7_step given no workspace.
+    a.err = record_dev != nullptr ? &record_dev->pad[0] : nullptr;
     a.count = reinterpret_cast<unsigned*>(base + 4);
     a.partials = reinterpret_cast<double*>(base + kHeader);
     cudaError_t e;

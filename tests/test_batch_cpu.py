@@ -36,6 +36,13 @@ def test_plane_independent_laws_stack_equal_shapes():
     "field T init 0 range -1 1\nterm t\n  d T = -T * rim\n",              # `rim` marks the lattice's z faces
     "field T init 0 range -1 1\nterm t\n  d T = -T + maxof(T)\n",         # a lattice-wide reduction
     text("ops_fields.law"),                                               # distance and poisson
+    # A pointwise classical term whose learned equations read across planes (ldiffuse's faces along z): learned
+    # schemes may be turned on after planning, so the instances stay apart.
+    "field T init 290 range 0 6000\nparam k = 1\nnet lh in 5 hidden 8 out 4 act tanh file none\n"
+    "term t\n  d T = -k * T\n  learned d T = ldiffuse(lh, k, T)\n",
+    # A pointwise learned term whose learned step limit reduces over the lattice.
+    "field T init 1 range -10 10\nterm t\n  d T = -T\n  learned d T = -2 * T\n"
+    "  learned max_dt = 0.1 / (maxof(T) + 1)\n",
 ])
 def test_laws_that_couple_planes_keep_instances_apart(law):
     assert plan(law, UNEVEN) == (5, False, [0, 1, 2, 3, 4], [0, 0, 0, 0, 0])

@@ -56,6 +56,53 @@ def test_noalloc_matches_workspace_step_two_calls_in_a_row(cuda):
             c, d = d, c
 
 
+def test_noalloc_without_contracts_matches_and_reports_into_its_record(cuda):
+    """check == 0: the field must still equal fe_heat7_step's bit for bit. A TMA variant still takes a record, for the
+    kernel's error word: the call clears whatever the record held before (here stale nonzero bytes) and a clean pass
+    leaves it all zero. Without a record a TMA variant is refused; the plain kernel (no waits) runs without one."""
+    import torch
+    from fieldcuda import _lib, kernels
+    lib = _lib.lib()
+    shape = (20, 36, 128)  # (nz, ny, nx)
+    nz, ny, nx = shape
+    T0 = np.random.default_rng(12).uniform(-1.0, 3.0, shape).astype(np.float32)
+    k, h, dt = 1.3, 0.25, 0.004
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for variant, zchunk in ((1, 5), (0, 8), (-1, 7)):
+        a = torch.from_numpy(T0).cuda()
+        b = torch.empty_like(a)
+        ws = kernels.heat7_workspace(shape, variant, zchunk)
+        want = []
+        for _ in range(2):
+            kernels.check_reset(ws)
+            kernels.heat7_step(a, b, k, h, dt, variant=variant, zchunk=zchunk, check=0, workspace=ws)
+            want.append(b.clone())
+            a, b = b, a
+        c = torch.from_numpy(T0).cuda()
+        d = torch.empty_like(c)
+        rec_dev = torch.full((ctypes.sizeof(_lib.fe_check),), 0xA5, dtype=torch.uint8, device="cuda")
+        for i in range(2):
+            _lib.check(lib.fe_heat7_step_noalloc(_ptr(c), _ptr(d), nx, ny, nz, k, h, dt, -1e30, 1e30, variant, zchunk,
+                                                 0, _ptr(rec_dev), s))
+            torch.cuda.synchronize()
+            assert torch.equal(d.view(torch.int32), want[i].view(torch.int32)), (variant, i)
+            assert int(rec_dev.count_nonzero()) == 0, (variant, i)  # cleared, and no error word
+            rec_dev.fill_(0x5A)
+            c, d = d, c
+        if variant >= 0:
+            status = lib.fe_heat7_step_noalloc(_ptr(c), _ptr(d), nx, ny, nz, k, h, dt, -1e30, 1e30, variant, zchunk, 0,
+                                               None, s)
+            assert status == _lib.FE_EINVAL and "record" in _lib.last_error()
+        else:
+            # A third step from the second's result, without a record, against the workspace form of that step.
+            third = torch.empty_like(c)
+            kernels.heat7_step(c, third, k, h, dt, variant=variant, zchunk=zchunk, check=0, workspace=None)
+            _lib.check(lib.fe_heat7_step_noalloc(_ptr(c), _ptr(d), nx, ny, nz, k, h, dt, -1e30, 1e30, variant, zchunk,
+                                                 0, None, s))
+            torch.cuda.synchronize()
+            assert torch.equal(d.view(torch.int32), third.view(torch.int32))
+
+
 def test_noalloc_refuses_sizes_beyond_its_scratch(cuda):
     import torch
     from fieldcuda import _lib
