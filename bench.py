@@ -248,6 +248,207 @@ def copy_roof_gbs(cells, stream, reps=10):
     return 2 * 4 * cells * reps / (e0.elapsed_time(e1) * 1e-3) / 1e9
 
 
+def pct(values, q):
+    import numpy as np
+    return float(np.percentile(np.asarray(values, dtype=np.float64), q))
+
+
+def step_times(s, dt, steps, stream_sync):
+    """Per-step times of `steps` steps of solver `s`: device time of each step (CUDA events on the solver's stream
+    around it; contracts checked on the card, judged after the run: lazy readback, nothing fetched) and the host's wall
+    time of each step when every step is judged on the host (its contract records read back: the wall time a caller
+    that waits for each step sees). Returns (device ms list, wall ms list, violations)."""
+    import torch
+    st = torch.cuda.ExternalStream(s.stream)
+    s.set_deferred(True)
+    for _ in range(3):
+        s.step(dt)
+    s.sync()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    stream_sync()
+    ev[0].record(st)
+    for i in range(steps):
+        s.step(dt)
+        ev[i + 1].record(st)
+    st.synchronize()
+    dev = [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]
+    s.sync()
+    broken = len(s.violations())
+    s.set_deferred(False)
+    wall = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        s.step(dt)
+        wall.append((time.perf_counter() - t0) * 1e3)
+        broken += len(s.violations())
+    return dev, wall, broken
+
+
+def stats(ms):
+    import numpy as np
+    return {"p50_ms": pct(ms, 50), "p99_ms": pct(ms, 99), "mean_ms": float(np.mean(ms))}
+
+
+C1_FIXTURE = os.path.join(ROOT, "tests", "golden", "large", "c1_heat_128.npz")
+
+
+def c1_section(stream_sync, peak):
+    """BASELINE's first configuration as stated: the heat law on 128^3 (h = 1/128, dt = 0.4 h^2 / 6, one substep),
+    4 seeded Gaussian blobs, 100 steps, contracts on. Per-step device and wall times, the engine against the
+    hand-written kernel (every step, to the bit), and the final state against the reference's CPU solver and against
+    the same scheme in FP64 (tests/golden/large/c1_heat_128.npz: both at its sampled cells and planes); the
+    reference's own OpenMP solver timed on the same steps on this host."""
+    import numpy as np
+    import torch
+    from fieldcuda import kernels
+    from fieldcuda.solver import Solver
+    from oracle import heat as oh
+    n, steps = 128, 100
+    h = 1.0 / n
+    dt = 0.4 * h * h / 6.0
+    T0 = oh.gaussian_blobs(n, h, seed=0)
+    s = Solver(HEAT_LAW, n, n, n, h, "heat.law")
+    s.set_field("T", T0)
+    a = torch.from_numpy(T0).cuda()
+    b = torch.empty_like(a)
+    eng = torch.empty_like(a)
+    ws = kernels.heat7_workspace(T0.shape, 0, 16)
+    st = torch.cuda.ExternalStream(s.stream)
+    dev, wall, same, broken = [], [], True, 0
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stream_sync()
+        t0 = time.perf_counter()
+        e0.record(st)
+        s.step(dt)          # judged on the host before it returns
+        e1.record(st)
+        wall.append((time.perf_counter() - t0) * 1e3)
+        st.synchronize()
+        dev.append(e0.elapsed_time(e1))
+        broken += len(s.violations())
+        kernels.heat7_step(a, b, 1.0, h, dt, variant=0, zchunk=16, check=0, workspace=ws)
+        a, b = b, a
+        s.fetch_device("T", eng)
+        torch.cuda.synchronize()
+        same = same and bool(torch.equal(eng.view(torch.int32), a.view(torch.int32)))
+    got = s.values("T").astype(np.float64)
+    d1 = s.digest()
+    s.close()
+    s = Solver(HEAT_LAW, n, n, n, h, "heat.law")
+    s.set_field("T", T0)
+    for _ in range(steps):
+        s.step(dt)
+    deterministic = s.digest() == d1
+    s.close()
+    out = {"lattice": "128^3", "steps": steps, "dt": dt, "device": stats(dev), "wall_judged_each_step": stats(wall),
+           "gbs_device_mean": BYTES_PER_CELL * n ** 3 / (stats(dev)["mean_ms"] * 1e-3) / 1e9,
+           "bit_identical_to_handwritten_every_step": same, "deterministic_two_runs": deterministic,
+           "violations": broken}
+    out["roofline_frac_mean_step"] = out["gbs_device_mean"] / peak
+    if os.path.exists(C1_FIXTURE):
+        z = np.load(C1_FIXTURE)
+        meta = json.loads(str(z["meta"]))
+        p = z["pick"]
+        ix = np.ix_(p, p, p)
+        out["rel_err_vs_reference_cpu"] = max(float(np.abs(got[ix] - z["ref_T"]).max()),
+                                              float(np.abs(got[z["planes"]] - z["refplanes_T"]).max())) / meta["max_abs"]["T"]
+        out["rel_err_vs_fp64"] = float(np.abs(got[ix] - z["fp64_T"]).max()) / meta["max_abs"]["fp64_T"]
+        out["reference_rel_err_vs_fp64"] = float(np.abs(z["ref_T"] - z["fp64_T"]).max()) / meta["max_abs"]["fp64_T"]
+        out["err_note"] = ("max |difference| / max |T| at the fixture's 4096 sampled cells (edges, quarter points, middle) "
+                           "and two full planes; the FP64 solve is the same scheme in double (tests/golden/make_golden.py)")
+    res = cpu_reference_heat(n, steps, 1, os.cpu_count() or 1)
+    if res is not None:
+        ms, kind, cores = res
+        out["cpu_baseline"] = {"value": ms, "unit": "ms/step", "cores": cores, "kind": kind,
+                               "sample": f"{steps} timed steps of the 128^3 heat law after 1 warm-up, reference lawc"}
+        out["speedup_vs_cpu_device_p50"] = ms / out["device"]["p50_ms"]
+    return out
+
+
+def c2_section(stream_sync, peak, cpu=True):
+    """BASELINE's second configuration: the heat law at 256^3 and 512^3 over 1000 steps, and the 43-term, 6-field law
+    (tests/laws/multifield43.law, seed 0) at 256^3 (1000 steps) and 512^3 (300 steps), with lazy readback (nothing
+    fetched; contracts checked on the card every step, judged after the run): p50/p99 of the per-step device time,
+    the wall time of a step judged on the host, effective bandwidth at the algorithmic bytes and its fraction of the
+    measured copy roof; the reference's OpenMP solver on the 43-term law at 256^3 on this host."""
+    import numpy as np
+    from fieldcuda.solver import Solver
+    from fieldcuda.workloads import multifield_bytes_per_cell, multifield_law
+    from oracle import heat as oh
+    out = {}
+    for n in (256, 512):
+        h = 1.0 / n
+        dt = 0.4 * h * h / 6.0
+        s = Solver(HEAT_LAW, n, n, n, h, "heat.law")
+        s.set_field("T", oh.gaussian_blobs(n, h, seed=0))
+        dev, wall, broken = step_times(s, dt, 1000, stream_sync)
+        s.close()
+        d = stats(dev)
+        gbs = BYTES_PER_CELL * n ** 3 / (d["mean_ms"] * 1e-3) / 1e9
+        out[f"heat_{n}"] = {"steps": 1000, "device": d, "wall_judged_each_step": stats(wall), "gbs": gbs,
+                            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "frac": gbs / peak,
+                                         "bytes_per_cell_step": BYTES_PER_CELL}, "violations": broken}
+    text, rw = multifield_law(0)
+    bpc = multifield_bytes_per_cell(rw)
+    for n, steps in ((256, 1000), (512, 300)):
+        h = 1.0 / n
+        dt = 0.1 * h * h
+        s = Solver(text, n, n, n, h, "multifield43.law")
+        rng = np.random.default_rng(43)
+        for i in range(6):
+            s.set_field(f"f{i}", rng.uniform(-1, 1, (n, n, n)).astype(np.float32))
+        s.step(dt)
+        launches = s.profile()["launches"]
+        passes = sum(s.last_substeps())
+        dev, wall, broken = step_times(s, dt, steps, stream_sync)
+        s.close()
+        d = stats(dev)
+        gbs = bpc * n ** 3 / (d["mean_ms"] * 1e-3) / 1e9
+        out[f"multifield43_{n}"] = {"steps": steps, "device": d, "wall_judged_each_step": stats(wall), "gbs": gbs,
+                                    "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "frac": gbs / peak,
+                                                 "bytes_per_cell_step": bpc},
+                                    "launches_per_step": launches, "term_passes_per_step": passes, "violations": broken}
+    if cpu:
+        res = cpu_reference_law(text, 256, 0.1 / 256 ** 2, 2, {f"f{i}": ("uniform", 43 + i) for i in range(6)})
+        if res is not None:
+            ms, cores = res
+            out["multifield43_256"]["cpu_baseline"] = {
+                "value": ms, "unit": "ms/step", "cores": cores, "kind": "reference",
+                "sample": "2 timed steps of the 43-term law at 256^3 after 1 warm-up, reference lawc"}
+            out["multifield43_256"]["speedup_vs_cpu_device_p50"] = ms / out["multifield43_256"]["device"]["p50_ms"]
+    out["note"] = ("device: CUDA events around every step on the solver's stream; wall: host time of a step judged on the "
+                   "host (its records read back). Multi-field bytes: per term 4 B a cell for every field it reads or "
+                   "writes plus 4 B for every field it writes (fieldcuda/workloads.py)")
+    return out
+
+
+def cpu_reference_law(text, n, dt, steps, fields):
+    """Times the reference's own OpenMP CPU solver (oracle/_ref/lawc) on law `text` at n^3: ms/step over `steps` after
+    one warm-up, all host cores. `fields`: name -> ("uniform", seed) starting states, U[-1, 1]. None without lawc."""
+    lawc = os.path.join(ROOT, "oracle", "_ref", "lawc")
+    if not os.path.exists(lawc):
+        return None
+    import numpy as np
+    threads = os.cpu_count() or 1
+    work = tempfile.mkdtemp(prefix="fe_cpu_")
+    try:
+        law = os.path.join(work, "law.law")
+        open(law, "w").write(text)
+        scene = os.path.join(work, "s.scene")
+        open(scene, "w").write(f"grid {n} {n} {n} {1.0 / n!r}\nlaw {law}\n")
+        init = os.path.join(work, "init")
+        os.makedirs(init)
+        for name, (_, seed) in fields.items():
+            np.random.default_rng(seed).uniform(-1, 1, (n, n, n)).astype(np.float32).tofile(os.path.join(init, name + ".bin"))
+        out = os.path.join(work, "t.json")
+        subprocess.run([lawc, "--scene", scene, "--init", init, "--steps", str(steps + 1), "--dt", repr(dt), "--json", out,
+                        "--warmup", "1"], check=True, env=dict(os.environ, OMP_NUM_THREADS=str(threads)),
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        return json.load(open(out))["mean_ms"], threads
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
 HESTON_EXPLICIT_LAW = os.path.join(ROOT, "tests", "laws", "heston_explicit.law")
 HESTON_CF = os.path.join(ROOT, "tests", "golden", "heston", "cf_2048.npz")
 HESTON_BUCKETS = ((128, 64), (256, 128), (512, 256))
@@ -665,6 +866,16 @@ def run_ours(args, world, rank, local):
     broken = judge()
     e2e_ms = max_over_ranks(world, (time.perf_counter() - t0) * 1e3)
     assert not broken, broken
+
+    # Bit-identical across runs: the same start stepped twice gives the same FNV-1a digest of the state.
+    digests = []
+    for _ in range(2):
+        upload()
+        for _ in range(10):
+            stepper.step(dt)
+        judge()
+        digests.append(s.digest())
+    deterministic = digests[0] == digests[1]
     s.close()
 
     side = torch.cuda.Stream()
@@ -694,6 +905,11 @@ def run_ours(args, world, rank, local):
             cpu = {"value": BYTES_PER_CELL * cells / (ms * 1e-3) / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
                    "sample": f"1 step of the {n}^3 heat law, numpy restatement (oracle/heat.py)"}
 
+    c1 = c2 = None
+    if world == 1 and not args.no_c1:
+        c1 = c1_section(torch.cuda.synchronize, peak)
+    if world == 1 and not args.no_c2:
+        c2 = c2_section(torch.cuda.synchronize, peak, cpu=not args.no_cpu)
     heston = None
     if not args.no_heston:
         heston = heston_batch_section(torch.cuda.synchronize)
@@ -724,7 +940,9 @@ def run_ours(args, world, rank, local):
                    "l2": "inputs larger than L2 (512 MiB a buffer)",
                    "handwritten_kernel_gbs": BYTES_PER_CELL * cells / (hand_ms * 1e-3) / 1e9},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "generated gather pass fe_pass_t0g (8 B/cell)",
+                     "traffic": traffic, "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of the same pass, "
+                     "copied from profiles/heat_gather_512.md (an ncu capture), not measured in this run",
+                     "kernel": "generated gather pass fe_pass_t0g (8 B/cell)",
                      "peak_source": f"{peak_kind} copy (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                      "copy_same_run_gbs": copy_gbs},
         "cpu_baseline": cpu,
@@ -734,6 +952,12 @@ def run_ours(args, world, rank, local):
                         "fe_law_fetch of the state to pinned host memory (wall clock)"},
         "gpu_launches": launches,
         "clocks": clk,
+        "deterministic": deterministic,
+        "err_vs_fp64": (c1 or {}).get("rel_err_vs_fp64"),
+        "err_vs_fp64_note": "C1 (128^3, 100 steps): max |T - T_fp64| / max |T_fp64| at the fixture's sampled cells, "
+                            "T_fp64 the same scheme in double",
+        "c1_128": c1,
+        "c2_lazy": c2,
         "heston_batch": heston,
         "multifield_256": multifield,
         "adjoint_calibration": calibration,
@@ -843,6 +1067,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=512)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-c1", action="store_true", help="skip the 128^3 x 100-step heat section")
+    ap.add_argument("--no-c2", action="store_true", help="skip the 256^3 / 512^3 lazy-readback section")
     ap.add_argument("--no-heston", action="store_true", help="skip the batched Heston ADI section")
     ap.add_argument("--no-multifield", action="store_true", help="skip the 43-term multi-field law section")
     ap.add_argument("--no-nets", action="store_true", help="skip the net ops section (fp32 and tensor-core nets)")

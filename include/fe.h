@@ -86,9 +86,9 @@ int fe_copy_f32(const float* src_dev, float* dst_dev, size_t n, void* stream);
  * zchunk). The caller passes the field buffers and a device fe_check `record_dev`, which the call clears and the pass
  * fills: needed with `check` (the contracts) and with a TMA variant (variant >= 0) even without `check`, since a
  * bounded wait that gives up raises the kernel's error word in record_dev->pad[0] (bit 1: a wait gave up; 0: none),
- * which the caller reads after the stream has run; optional for the plain kernel without `check`. The array is shared by every
- * call; each call clears what must start at zero, and calls that overlap on the GPU (several streams or host threads)
- * race on it: serialise them on one stream. The first call on a device looks up the array's device address (once per
+ * which the caller reads after the stream has run; optional for the plain kernel without `check`. The array is shared
+ * by every call; each call clears what must start at zero, and calls that overlap on the GPU (several streams or host
+ * threads) race on it: serialise them on one stream. The first call on a device looks up the array's device address (once per
  * device, with that device current); that first call may load the library's device code and with it create the
  * array, so make one call (for example on a one-cell lattice) before a region that may not allocate and before any
  * stream capture. The address is kept for the device's primary context: after cudaDeviceReset, or from another
@@ -231,7 +231,8 @@ int fe_law_term_idle(const fe_law* law, int term);
  * term's learned scheme was kept in the last step, 2 it was undone, 0 the classical scheme ran alone, -1 no such term. */
 int fe_law_set_learned(fe_law* law, int on);
 int fe_law_term_learned(const fe_law* law, int term);
-/* FNV-1a over every field's bits in declaration order (FieldSet::digest, src/field/Grid.cpp:60-77). */
+/* FNV-1a over each field's name and then its values' bits, in declaration order (FieldSet::digest,
+ * src/field/Grid.cpp:60-77): a state equal to the bit to a reference FieldSet gives the same digest. */
 int fe_law_digest(fe_law* law, uint64_t* out);
 /* The handle's stream (a cudaStream_t), for callers that order their own work after its steps. */
 int fe_law_stream(const fe_law* law, void** stream);

@@ -401,8 +401,11 @@ int fe_law_digest(fe_law* law, uint64_t* out)
     std::uint64_t h = 1469598103934665603ull;
     std::vector<float> host(law->engine.cells());
     std::string why;
+    // FieldSet::digest (src/field/Grid.cpp:60-74): each field's name, then its values' bits, in declaration order.
     for (size_t f = 0; f < law->engine.law().fields.size(); ++f) {
         if (!law->engine.fetch(static_cast<int>(f), host.data(), false, why)) return fe::fail(FE_ECUDA, why);
+        const std::string& name = law->engine.law().fields[f].name;
+        h = fe::fnv1a(name.data(), name.size(), h);
         h = fe::fnv1a(host.data(), host.size() * sizeof(float), h);
     }
     *out = h;

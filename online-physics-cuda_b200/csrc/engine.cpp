@@ -48,6 +48,7 @@ Engine::~Engine()
     if (counts_ != nullptr) cudaFree(counts_);
     if (flags_ != nullptr) cudaFree(flags_);
     if (snapshot_ != nullptr) cudaFree(snapshot_);
+    if (bounds_rec_ != nullptr) cudaFree(bounds_rec_);
     if (ev0_ != nullptr) cudaEventDestroy(ev0_);
     if (ev1_ != nullptr) cudaEventDestroy(ev1_);
     if (stream_ != nullptr) cudaStreamDestroy(stream_);
@@ -192,6 +193,7 @@ bool Engine::create(const std::vector<law::Source>& sources, int nx, int ny, int
     partial_doubles_ = partial_doubles;
     if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&partials_), partial_doubles * sizeof(double)), "cudaMalloc (partials)", why)) return false;
     if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&counts_), (FE_MAX_OUT + 4) * sizeof(unsigned)), "cudaMalloc (counters)", why)) return false;
+    if (!cuda_ok(cudaMalloc(reinterpret_cast<void**>(&bounds_rec_), sizeof(FeCheck)), "cudaMalloc (upload bounds)", why)) return false;
     if (!cuda_ok(cudaMemsetAsync(counts_, 0, (FE_MAX_OUT + 4) * sizeof(unsigned), stream_), "memset", why)) return false;
 
     param_host_ = law_.param_values;
@@ -426,25 +428,20 @@ bool Engine::upload(int field, const void* src, bool device, std::string& why)
     }
     if (!sync(why)) return false;
     const cudaMemcpyKind kind = device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    if (!cuda_ok(cudaMemcpyAsync(now_[static_cast<std::size_t>(field)], src, cells_ * sizeof(float), kind, stream_), "upload", why)) return false;
+    float* dst = now_[static_cast<std::size_t>(field)];
+    if (!cuda_ok(cudaMemcpyAsync(dst, src, cells_ * sizeof(float), kind, stream_), "upload", why)) return false;
+    // The bounds of what arrived, for the idle-term test (CudaSolver.cpp:820-920 looks over uploaded planes the same
+    // way), taken on the card once the cells are there: one read at HBM rate instead of a host loop over every cell.
+    FeCheck* rec = bounds_rec_;
+    if (!cuda_ok(cudaMemsetAsync(rec, 0, sizeof(FeCheck), stream_), "upload bounds", why)) return false;
+    if (!cuda_ok(launch_bounds(dst, cells_, rec, sms_, stream_), "upload bounds", why)) return false;
+    FeCheck got{};
+    if (!cuda_ok(cudaMemcpyAsync(&got, rec, sizeof(FeCheck), cudaMemcpyDeviceToHost, stream_), "upload bounds", why)) return false;
+    // The caller's buffer is read only during the call: wait for the copy (and the 8 bytes of keys).
     if (!cuda_ok(cudaStreamSynchronize(stream_), "upload", why)) return false;
-    Bounds b{std::numeric_limits<double>::infinity(), -std::numeric_limits<double>::infinity()};
-    if (!device) {
-        // What the host writes it has at hand: its bounds, for the idle-term test (CudaSolver.cpp:820-920 looks over
-        // uploaded planes the same way).
-        const float* v = static_cast<const float*>(src);
-        float lo = std::numeric_limits<float>::infinity(), hi = -lo;
-        for (std::size_t i = 0; i < cells_; ++i) {
-            const float x = v[i];
-            if (x != x) continue;
-            lo = std::min(lo, x);
-            hi = std::max(hi, x);
-        }
-        b = Bounds{lo, hi};
-        if (lo > hi) b = Bounds{};
-    } else {
-        b = Bounds{};
-    }
+    Bounds b{};
+    const unsigned lo_key = ~got.lo_inv;
+    if (got.hi_key != 0u && lo_key != 0xffffffffu) b = Bounds{key_to_float(lo_key), key_to_float(got.hi_key)};
     bounds_[static_cast<std::size_t>(field)] = b;
     zero_[static_cast<std::size_t>(field)] = (b.lo == 0.0 && b.hi == 0.0) ? 1 : 0;
     carry_[static_cast<std::size_t>(field)] = Carry{};

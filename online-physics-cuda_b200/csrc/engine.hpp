@@ -172,6 +172,7 @@ private:
     std::size_t partial_doubles_ = 0;
     unsigned* counts_ = nullptr; // FE_MAX_OUT counters, then the error word
     unsigned* flags_ = nullptr;  // change flags of the distance and poisson ops
+    FeCheck* bounds_rec_ = nullptr; // the bounds of an upload (lo_inv / hi_key keys)
     std::vector<PendingStep> pending_;
     std::vector<double> param_host_;
     bool params_dirty_ = true;

@@ -52,6 +52,48 @@ __global__ void __launch_bounds__(256) totals_f32(const float* __restrict__ v, s
     fe_acc_finish(partials, static_cast<int>(gridDim.x), count, scratch, rec, true, false);
 }
 
+// The least and largest value of n cells (NaN left out, infinities kept) into rec->lo_inv / hi_key as ordered keys,
+// the contract record's convention (rec must start all zero). Min and max are exact and integer atomics land in any
+// order, so the answer does not depend on the schedule. For what an upload brings: the idle-term test needs the
+// bounds of every field it reads, and the uploaded cells are already on the card.
+__global__ void __launch_bounds__(256) bounds_f32(const float* __restrict__ v, size_t n, FeCheck* rec)
+{
+    const size_t head = min(n, static_cast<size_t>(((16u - (reinterpret_cast<size_t>(v) & 15u)) & 15u) / 4u));
+    const float* w = v + head;
+    const size_t m4 = (n - head) / 4;
+    const float4* w4 = reinterpret_cast<const float4*>(w);
+    float lo = __int_as_float(0x7f800000), hi = __int_as_float(0xff800000);
+    const size_t tid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    if (tid < head) {
+        lo = fminf(lo, v[tid]);
+        hi = fmaxf(hi, v[tid]);
+    }
+#pragma unroll 4
+    for (size_t i = tid; i < m4; i += stride) {
+        const float4 x = __ldg(w4 + i);
+        lo = fminf(fminf(lo, x.x), fminf(x.y, fminf(x.z, x.w)));
+        hi = fmaxf(fmaxf(hi, x.x), fmaxf(x.y, fmaxf(x.z, x.w)));
+    }
+    for (size_t i = 4 * m4 + tid; i < n - head; i += stride) {
+        lo = fminf(lo, w[i]);
+        hi = fmaxf(hi, w[i]);
+    }
+    // fminf/fmaxf return the other operand for a NaN, so a thread that saw only NaNs keeps lo > hi: nothing seen.
+    const unsigned klo = fe_warp_min(lo <= hi ? fe_order_key(lo) : 0xffffffffu);
+    const unsigned khi = fe_warp_max(lo <= hi ? fe_order_key(hi) : 0u);
+    if ((threadIdx.x & 31) == 0) {
+        if (klo != 0xffffffffu) atomicMax(&rec->lo_inv, ~klo);
+        if (khi != 0u) atomicMax(&rec->hi_key, khi);
+    }
+}
+
+cudaError_t launch_bounds(const float* v, size_t n, FeCheck* rec, int sms, cudaStream_t stream)
+{
+    bounds_f32<<<4 * sms, 256, 0, stream>>>(v, n, rec);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_totals(const float* v, size_t n, FeCheck* rec, double* partials, unsigned* count, cudaStream_t stream)
 {
     totals_f32<<<kTotalsBlocks, 256, 0, stream>>>(v, n, rec, partials, count);

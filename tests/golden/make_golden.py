@@ -227,6 +227,105 @@ def vjp_fixture(lawc):
         shutil.rmtree(work, ignore_errors=True)
 
 
+def pick(n):
+    """The sampled coordinates along an axis of n cells for the fixtures of large lattices: both edges, the quarter
+    points and the middle, each with a neighbour either side (16 values at n = 128)."""
+    q = [0, 1, 2, 3, n // 4 - 1, n // 4, n // 4 + 1, n // 2 - 1, n // 2, n // 2 + 1, 3 * n // 4 - 1, 3 * n // 4,
+         n - 4, n - 3, n - 2, n - 1]
+    return np.array(sorted(set(i for i in q if 0 <= i < n)), np.int64)
+
+
+def heat_fp64(T, D, h, dt, steps):
+    """The heat law's explicit scheme (acc = sum over present faces of (neighbour - cell), T += max(D, 0) acc / h^2 dt)
+    in FP64 arithmetic and storage: the FP64 solve the FP32 step's error is stated against."""
+    from oracle.heat import _faces
+    v = np.asarray(T, np.float64)
+    for _ in range(steps):
+        acc = np.zeros_like(v)
+        for nb, valid in _faces(v):
+            acc += np.where(valid, nb - v, 0.0)
+        v = v + max(D, 0.0) * acc / (h * h) * dt
+    return v
+
+
+def large_fixtures(lawc):
+    """The benchmarked lattices, pinned to the reference (lawc) at their full size: too large to commit whole, so each
+    fixture keeps the cells on a 16 x 16 x 16 grid of sampled coordinates (pick(n) per axis: edges, quarter points,
+    middle), the reference's FNV-1a digest of its final state and the largest |value|; c1_heat_128 also two full planes
+    (z = 0 and 64).
+
+    c1_heat_128: the heat law (tests/laws/heat.law) on 128^3, h = 1/128, dt = 0.4 h^2 / 6 (one substep), the sum of 4
+      Gaussian blobs from oracle.heat.gaussian_blobs(128, h, seed=0), 100 steps, contracts on; plus the same scheme in
+      FP64 (heat_fp64) sampled the same way.
+    multifield43_128: the 43-term law (tests/laws/multifield43.law) on 128^3, h = 1/128, dt = 0.1 h^2, 3 steps, fields
+      f0..f5 drawn U[-1, 1] in order from numpy default_rng(4343)."""
+    from oracle.heat import gaussian_blobs
+    n = 128
+    h = 1.0 / n
+    p = pick(n)
+    ix = np.ix_(p, p, p)
+    planes = np.array([0, n // 2], np.int64)
+    rng = np.random.default_rng(4343)
+    specs = [
+        dict(name="c1_heat_128", law="heat.law", dt=0.4 * h * h / 6.0, steps=100,
+             fields={"T": gaussian_blobs(n, h, seed=0)}),
+        dict(name="multifield43_128", law="multifield43.law", dt=0.1 * h * h, steps=3,
+             fields={f"f{i}": rng.uniform(-1, 1, (n, n, n)).astype(np.float32) for i in range(6)}),
+    ]
+    for spec in specs:
+        work = tempfile.mkdtemp(prefix="fe_large_")
+        try:
+            law = os.path.join(LAWS, spec["law"])
+            scene = os.path.join(work, "scene")
+            with open(scene, "w") as fh:
+                fh.write(f"grid {n} {n} {n} {h!r}\nlaw {law}\n")
+            init = os.path.join(work, "init")
+            os.makedirs(init)
+            for name, arr in spec["fields"].items():
+                np.ascontiguousarray(arr, np.float32).tofile(os.path.join(init, name + ".bin"))
+            dump, js = os.path.join(work, "dump"), os.path.join(work, "t.json")
+            subprocess.run([lawc, "--scene", scene, "--init", init, "--steps", str(spec["steps"]), "--dt", repr(spec["dt"]),
+                            "--dump", dump, "--every", str(spec["steps"]), "--json", js], check=True, capture_output=True,
+                           cwd=ROOT, env=dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 4)))
+            last = os.path.join(dump, f"step_{spec['steps']}")
+            meta_dump = json.load(open(os.path.join(last, "meta.json")))
+            timing = json.load(open(js))
+            arrays = {"pick": p, "planes": planes}
+            digest = 0xcbf29ce484222325
+            maxabs = {}
+            for f in meta_dump["fields"]:
+                final = np.fromfile(os.path.join(last, f + ".bin"), np.float32).reshape(n, n, n)
+                arrays[f"ref_{f}"] = final[ix]
+                if spec["name"] == "c1_heat_128":
+                    arrays[f"refplanes_{f}"] = final[planes]
+                maxabs[f] = float(np.abs(final).max())
+                digest = _fnv1a(f.encode(), digest)
+                digest = _fnv1a(np.ascontiguousarray(final, np.float32).view(np.uint8).tobytes(), digest)
+            if spec["name"] == "c1_heat_128":
+                v64 = heat_fp64(spec["fields"]["T"], 1.0, h, spec["dt"], spec["steps"])
+                arrays["fp64_T"] = v64[ix]
+                maxabs["fp64_T"] = float(np.abs(v64).max())
+            meta = dict(name=spec["name"], law=spec["law"], n=n, h=h, dt=spec["dt"], steps=spec["steps"],
+                        substeps=timing["substeps"], violations=timing["violations"], fields=meta_dump["fields"],
+                        ref_digest=f"{digest:016x}", max_abs=maxabs,
+                        made_by=f"the reference's lawc (its OpenMP CPU Solver), OMP_NUM_THREADS={os.cpu_count() or 4}")
+            os.makedirs(os.path.join(HERE, "large"), exist_ok=True)
+            np.savez_compressed(os.path.join(HERE, "large", spec["name"] + ".npz"), meta=json.dumps(meta), **arrays)
+            print(spec["name"], "substeps", meta["substeps"], "violations", meta["violations"], "digest", meta["ref_digest"])
+        finally:
+            shutil.rmtree(work, ignore_errors=True)
+
+
+def _fnv1a(data, h):
+    """FNV-1a 64 over `data` (bytes), continuing from h (FieldSet::digest mixes each field's name, then its values'
+    bits, in declaration order)."""
+    prime = 0x100000001b3
+    mask = (1 << 64) - 1
+    for b in data:
+        h = ((h ^ b) * prime) & mask
+    return h
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--lawc", default=os.path.join(ROOT, "oracle", "_ref", "lawc"))
@@ -234,9 +333,13 @@ def main():
     args = ap.parse_args()
     if not os.path.exists(args.lawc):
         sys.exit(f"no reference solver at {args.lawc}: build it with `make -C oracle ref`")
+    if args.only == "large":
+        large_fixtures(args.lawc)
+        return
     ir_fixtures(args.lawc)
     scene_fixtures(args.lawc)
     vjp_fixture(args.lawc)
+    large_fixtures(args.lawc)
     for case in cases():
         if args.only and case["name"] not in args.only.split(","):
             continue

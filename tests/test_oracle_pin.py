@@ -53,6 +53,25 @@ def test_heat_restatement_matches_the_law_oracle():
     assert np.array_equal(s.fields["T"].view(np.uint32), oh.cpu_step(T0, 1.0, h, dt).view(np.uint32))
 
 
+def test_c1_fixture_against_the_fp32_restatement():
+    """The full-size heat fixture (128^3, 100 steps; tests/golden/large/c1_heat_128.npz, made by the reference's lawc)
+    against the restatement of the generated kernel's FP32 arithmetic over the same 100 steps: within the 1e-6 the GPU
+    test holds the engine to, and the FP64 solve in the fixture within the same bound of both."""
+    from oracle import heat as oh
+    z = np.load(os.path.join(ROOT, "tests", "golden", "large", "c1_heat_128.npz"))
+    meta = json.loads(str(z["meta"]))
+    n, h, dt = meta["n"], meta["h"], meta["dt"]
+    T = oh.gaussian_blobs(n, h, seed=0)
+    for _ in range(meta["steps"]):
+        T = oh.gpu_order_step(T, 1.0, h, dt)
+    p = z["pick"]
+    ix = np.ix_(p, p, p)
+    assert float(np.abs(T[ix].astype(np.float64) - z["ref_T"]).max()) / meta["max_abs"]["T"] <= 1e-6
+    assert float(np.abs(T[z["planes"]].astype(np.float64) - z["refplanes_T"]).max()) / meta["max_abs"]["T"] <= 1e-6
+    assert float(np.abs(T[ix].astype(np.float64) - z["fp64_T"]).max()) / meta["max_abs"]["fp64_T"] <= 1e-6
+    assert float(np.abs(z["ref_T"].astype(np.float64) - z["fp64_T"]).max()) / meta["max_abs"]["fp64_T"] <= 1e-6
+
+
 def test_reverse_pass_reproduces_the_reference_vjp():
     """The adjoint law this backend builds (fe_law_adjoint), run by the oracle back over every kept state, against the
     reference's own lawc --vjp on the same scene and seed (tests/golden/scene/heat_vjp.npz): bit for bit, for the
