@@ -227,6 +227,50 @@ def vjp_fixture(lawc):
         shutil.rmtree(work, ignore_errors=True)
 
 
+BAD_LAWS = [
+    "field T init 0\nterm t\n  d T = (T + 1\n",
+    "field T init 0\nterm t\n  d T = T +* 2\n",
+    "field T init 0\nterm t\n  d T = nosuch(T)\n",
+    "field T init 0\nterm t\n  d T = shift(T, 0.5, 0, 0)\n",
+    "field T init 0\nterm t\n  d T = T 2\n",
+    "field T init 0\nparam p = T\nterm t\n  d T = p\n",
+    "field T init 0\nterm t\n  let h = 2\n  d T = 1\n",
+    "field T init 0\nterm t\n  d T = min(T)\n",
+    "field T init 0 range 2 1\nterm t\n  d T = 1\n",
+    "field T init 0\nterm t\n  max_dt = dt\n  d T = 1\n",
+    "field T init 0\nterm t\n  max_dt = T\n  d T = 1\n",
+    "field T init 0\nfield T init 1\nterm t\n  d T = 1\n",
+    "field T init 0 static\nterm t\n  d T = 1\n  conserves Q\n",
+    "field T init 0\nd T = 1\nterm t\n  learned d T = 2\n  d T = 1 +\n",
+    "field T init 0\nderive A = T\nderive A = 2 * T\nterm t\n  d T = 1 ^\n",
+    "field T init 0\nnet n1 in 3 out 1 act tanh file none\nterm t\n  d T = mlp(n1, T, T)\n",
+    "field T init 0\nnet n1 in 2 hidden 200 out 1 act tanh\nterm t\n  d T = flux(n2, T)\n",
+    "field T init 0\nterm t\n  d T = poisson(T, 0) + 1 2\n  bogus line\n",
+    "field T init 0\nterm t\n  d T = @\n",
+    "field T init 0\nterm t\nterm t\n  d T = 1\n  conserves T + T\n",
+]
+
+
+def error_fixtures(lawc):
+    """The reference's lawc on malformed laws: the error lines it prints (source name replaced by 'law'), which the
+    law front end must give word for word (tests/test_ir_cpu.py)."""
+    out = []
+    work = tempfile.mkdtemp(prefix="fe_err_")
+    try:
+        path = os.path.join(work, "bad.law")
+        for text in BAD_LAWS:
+            with open(path, "w") as f:
+                f.write(text)
+            res = subprocess.run([lawc, "--ir", path], capture_output=True, text=True)
+            lines = [l.replace(path + ":", "law:") for l in (res.stdout + res.stderr).splitlines() if l.startswith(path + ":")]
+            out.append({"law": text, "errors": lines, "rc": res.returncode})
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+    with open(os.path.join(HERE, "law_errors.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print("errors", len(out))
+
+
 def pick(n):
     """The sampled coordinates along an axis of n cells for the fixtures of large lattices: both edges, the quarter
     points and the middle, each with a neighbour either side (16 values at n = 128)."""
@@ -336,7 +380,11 @@ def main():
     if args.only == "large":
         large_fixtures(args.lawc)
         return
+    if args.only == "errors":
+        error_fixtures(args.lawc)
+        return
     ir_fixtures(args.lawc)
+    error_fixtures(args.lawc)
     scene_fixtures(args.lawc)
     vjp_fixture(args.lawc)
     large_fixtures(args.lawc)

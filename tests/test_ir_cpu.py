@@ -47,6 +47,21 @@ def test_reference_bench_laws_lower_identically():
         assert mine == ref, paths
 
 
+def test_law_errors_match_the_reference_word_for_word():
+    """Malformed laws give the reference lawc's own error lines, in its order (tests/golden/law_errors.json, made by
+    it): the messages are part of the language's interface."""
+    from fieldcuda import _lib, solver
+    cases = json.load(open(os.path.join(ROOT, "tests", "golden", "law_errors.json")))
+    assert len(cases) >= 20
+    for case in cases:
+        assert case["rc"] != 0 and case["errors"]
+        with pytest.raises(_lib.FeError) as e:
+            solver.ir_json(case["law"])
+        got = [line for line in str(e.value).splitlines() if line.startswith("law:") or "] law:" in line]
+        got = [line[line.index("law:"):] for line in got]
+        assert got == case["errors"], case["law"]
+
+
 def test_law_errors_name_the_line():
     from fieldcuda import _lib, solver
     with pytest.raises(_lib.FeError) as e:
