@@ -88,9 +88,9 @@ int fe_copy_f32(const float* src_dev, float* dst_dev, size_t n, void* stream);
  * bounded wait that gives up raises the kernel's error word in record_dev->pad[0] (bit 1: a wait gave up; 0: none),
  * which the caller reads after the stream has run; optional for the plain kernel without `check`. The array is shared
  * by every call; each call clears what must start at zero, and calls that overlap on the GPU (several streams or host
- * threads) race on it: serialise them on one stream. The first call on a device looks up the array's device address (once per
- * device, with that device current); that first call may load the library's device code and with it create the
- * array, so make one call (for example on a one-cell lattice) before a region that may not allocate and before any
+ * threads) race on it: serialise them on one stream. The first call on a device looks up the array's device address
+ * (once per device, with that device current); that first call may load the library's device code and with it create
+ * the array, so make one call (for example on a one-cell lattice) before a region that may not allocate and before any
  * stream capture. The address is kept for the device's primary context: after cudaDeviceReset, or from another
  * context, it is stale. Nothing here calls cudaMalloc or cudaFree. */
 int fe_heat7_step_noalloc(const float* T_dev, float* out_dev, int nx, int ny, int nz, float k, float h, float dt, float lo,
@@ -151,6 +151,15 @@ typedef struct fe_field_info {
  * backend does not run. Replaces CudaSolver::create (src/field/cuda/CudaSolver.hpp:27, CudaSolver.cpp:1143-1152). */
 int fe_law_create(const char* law_text, const char* source_name, int nx, int ny, int nz, double h, fe_law** out);
 void fe_law_destroy(fe_law* law);
+/* The same from the law's IR as the reference writes it (ir::to_json, src/field/ir/LawIR.cpp:528-593; lawc --ir-json):
+ * for a host that holds a compiled Law rather than its text (the reference's CudaSolver::create takes a Law and lowers
+ * it, CudaSolver.cpp:122). Nets' weights are read from the files the JSON names (the untrained start when a net has
+ * none). The IR must lower back to itself here (same instructions and programs), else FE_ELAW. fe_law_ir_check does the
+ * rebuilding and lowering without a device and writes this backend's JSON of it (text as for fe_law_ir_json). */
+int fe_law_create_ir(const char* ir_json, int nx, int ny, int nz, double h, fe_law** out);
+int fe_law_ir_check(const char* ir_json, char* buf, size_t cap, size_t* needed);
+/* fe_law_source for a law given as its IR JSON (CudaSolver::source, src/field/cuda/CudaSolver.hpp:32). */
+int fe_law_source_ir(const char* ir_json, int nx, int ny, int nz, double h, char* buf, size_t cap, size_t* needed);
 
 /* Compile-only services, no device needed: the IR as the reference's JSON (lawc --ir-json, src/field/ir/LawIR.cpp:528-593)
  * or listing (lawc --ir, LawIR.cpp:595-656), and the generated CUDA translation unit (lawc --cuda, CudaSolver::source).
@@ -184,6 +193,17 @@ int fe_law_upload(fe_law* law, int field, const float* host);
 int fe_law_upload_device(fe_law* law, int field, const float* dev);
 int fe_law_fetch(fe_law* law, int field, float* host);
 int fe_law_fetch_device(fe_law* law, int field, float* dev);
+/* Part of a field from the host array of the whole field (nx*ny*nz floats, x fastest): only the box [x0, x1) x [y0, y1)
+ * x [z0, z1), or only the z-planes whose flag in `planes` (nz bytes) is set. The edits of the reference's host FieldSet
+ * (FieldEdits::planes and ::boxes, src/field/Backend.hpp:28-40; the uploads of CudaSolver.cpp:779-920). */
+int fe_law_upload_box(fe_law* law, int field, const float* host, int x0, int y0, int z0, int x1, int y1, int z1);
+int fe_law_upload_planes(fe_law* law, int field, const float* host, const unsigned char* planes);
+/* The window moved by (dx, dy, dz) cells (FieldEdits::shift, Backend.hpp:31-39; Solver::shift_window): the cell now at c
+ * holds what was at c + d. Every field, and what distance and poisson keep from step to step (seeds, warm start),
+ * moves on the card, the cells that left wrapping round to the side that arrives, as the reference's ring-addressed
+ * lattice reads them after its origin moves (CudaCodegen.cpp:45-51); the caller then uploads the arriving boxes
+ * (fe_law_upload_box). Here the cells move once a shift, at HBM rate, so that no kernel pays ring addressing every step. */
+int fe_law_shift(fe_law* law, int dx, int dy, int dz);
 /* The card's current buffer of a field (valid until the next step). */
 /* The field's current device buffer was changed in place by the caller, on the handle's stream (fe_law_stream) after
  * its last step: the backend forgets what it knew of the field's bounds (no counterpart in the reference, whose host

@@ -4,6 +4,7 @@
 #include "adjoint.hpp"
 #include "api_common.hpp"
 #include "engine.hpp"
+#include "ir_json.hpp"
 
 #include <cstring>
 #include <memory>
@@ -79,6 +80,37 @@ int fe_law_create(const char* law_text, const char* source_name, int nx, int ny,
     return fe::ok();
 }
 
+int fe_law_create_ir(const char* ir_json, int nx, int ny, int nz, double h, fe_law** out)
+{
+    if (ir_json == nullptr || out == nullptr) return fe::fail(FE_EINVAL, "fe_law_create_ir: null argument");
+    *out = nullptr;
+    fe::law::Law law;
+    fe::ir::Module m;
+    std::string why;
+    if (!fe::law_from_ir_json(ir_json, law, m, why)) return fe::fail(FE_ELAW, why);
+    auto l = std::make_unique<fe_law>();
+    if (!l->engine.create(std::move(law), std::move(m), nx, ny, nz, h, why)) {
+        int code = FE_ECUDA;
+        if (why.find("does not run") != std::string::npos || why.find("at most") != std::string::npos) code = FE_EUNSUP;
+        else if (why.find("no CUDA device") != std::string::npos || why.find("built for sm_100a") != std::string::npos ||
+            why.find("entry point") != std::string::npos) code = FE_ENODEV;
+        else if (why.find("lattice needs") != std::string::npos || why.find("2^32") != std::string::npos) code = FE_EINVAL;
+        return fe::fail(code, why);
+    }
+    *out = l.release();
+    return fe::ok();
+}
+
+int fe_law_ir_check(const char* ir_json, char* buf, size_t cap, size_t* needed)
+{
+    if (ir_json == nullptr) return fe::fail(FE_EINVAL, "fe_law_ir_check: null argument");
+    fe::law::Law law;
+    fe::ir::Module m;
+    std::string why;
+    if (!fe::law_from_ir_json(ir_json, law, m, why)) return fe::fail(FE_ELAW, why);
+    return put_text(fe::ir::to_json(m, law), buf, cap, needed);
+}
+
 void fe_law_destroy(fe_law* law)
 {
     delete law;
@@ -119,6 +151,19 @@ int fe_law_source(const char* law_text, int nx, int ny, int nz, double h, char* 
     if (!compile_law(law_text, law, why)) return fe::fail(FE_ELAW, why);
     if (nx < 1 || ny < 1 || nz < 1 || !(h > 0.0)) return fe::fail(FE_EINVAL, "bad lattice");
     const fe::ir::Module m = fe::ir::lower(law);
+    fe::gen::Plan plan;
+    if (!fe::gen::generate(m, law, nx, ny, nz, h, plan, why)) return fe::fail(FE_EUNSUP, why);
+    return put_text(plan.source, buf, cap, needed);
+}
+
+int fe_law_source_ir(const char* ir_json, int nx, int ny, int nz, double h, char* buf, size_t cap, size_t* needed)
+{
+    if (ir_json == nullptr) return fe::fail(FE_EINVAL, "fe_law_source_ir: null argument");
+    if (nx < 1 || ny < 1 || nz < 1 || !(h > 0.0)) return fe::fail(FE_EINVAL, "bad lattice");
+    fe::law::Law law;
+    fe::ir::Module m;
+    std::string why;
+    if (!fe::law_from_ir_json(ir_json, law, m, why)) return fe::fail(FE_ELAW, why);
     fe::gen::Plan plan;
     if (!fe::gen::generate(m, law, nx, ny, nz, h, plan, why)) return fe::fail(FE_EUNSUP, why);
     return put_text(plan.source, buf, cap, needed);
@@ -216,6 +261,31 @@ int fe_law_upload_device(fe_law* law, int field, const float* dev)
     std::string why;
     if (!field_ok(law, field) || dev == nullptr) return fe::fail(FE_EINVAL, "fe_law_upload_device: bad field or pointer");
     if (!law->engine.upload(field, dev, true, why)) return fe::fail(FE_ECUDA, why);
+    return fe::ok();
+}
+
+int fe_law_shift(fe_law* law, int dx, int dy, int dz)
+{
+    std::string why;
+    if (law == nullptr) return fe::fail(FE_EINVAL, "fe_law_shift: null handle");
+    if (!law->engine.shift(dx, dy, dz, why)) return fe::fail(FE_ECUDA, why);
+    return fe::ok();
+}
+
+int fe_law_upload_box(fe_law* law, int field, const float* host, int x0, int y0, int z0, int x1, int y1, int z1)
+{
+    std::string why;
+    if (!field_ok(law, field) || host == nullptr) return fe::fail(FE_EINVAL, "fe_law_upload_box: bad field or pointer");
+    const int box[6] = {x0, y0, z0, x1, y1, z1};
+    if (!law->engine.upload_box(field, host, box, why)) return fe::fail(FE_ECUDA, why);
+    return fe::ok();
+}
+
+int fe_law_upload_planes(fe_law* law, int field, const float* host, const unsigned char* planes)
+{
+    std::string why;
+    if (!field_ok(law, field) || host == nullptr || planes == nullptr) return fe::fail(FE_EINVAL, "fe_law_upload_planes: bad field or pointer");
+    if (!law->engine.upload_planes(field, host, planes, why)) return fe::fail(FE_ECUDA, why);
     return fe::ok();
 }
 

@@ -49,6 +49,7 @@ Engine::~Engine()
     if (flags_ != nullptr) cudaFree(flags_);
     if (snapshot_ != nullptr) cudaFree(snapshot_);
     if (bounds_rec_ != nullptr) cudaFree(bounds_rec_);
+    if (rotate_scratch_ != nullptr) cudaFree(rotate_scratch_);
     if (ev0_ != nullptr) cudaEventDestroy(ev0_);
     if (ev1_ != nullptr) cudaEventDestroy(ev1_);
     if (stream_ != nullptr) cudaStreamDestroy(stream_);
@@ -70,14 +71,34 @@ bool Engine::create(const std::vector<law::Source>& sources, int nx, int ny, int
     h_ = h;
     cells_ = static_cast<std::size_t>(nx) * ny * nz;
     std::vector<std::string> errors;
-    law_ = law::compile(sources, errors);
+    law::Law law = law::compile(sources, errors);
     if (!errors.empty()) {
         std::ostringstream all;
         for (const std::string& e : errors) all << e << "\n";
         why = all.str();
         return false;
     }
-    mod_ = ir::lower(law_);
+    ir::Module m = ir::lower(law);
+    return create(std::move(law), std::move(m), nx, ny, nz, h, why);
+}
+
+bool Engine::create(law::Law law, ir::Module module, int nx, int ny, int nz, double h, std::string& why)
+{
+    if (nx < 1 || ny < 1 || nz < 1 || !(h > 0.0)) {
+        why = "the lattice needs nx, ny, nz >= 1 and h > 0";
+        return false;
+    }
+    if (static_cast<unsigned long long>(nx) * ny * nz >= 0xffffffffull) {
+        why = "more than 2^32 - 1 cells";
+        return false;
+    }
+    nx_ = nx;
+    ny_ = ny;
+    nz_ = nz;
+    h_ = h;
+    cells_ = static_cast<std::size_t>(nx) * ny * nz;
+    law_ = std::move(law);
+    mod_ = std::move(module);
     if (!gen::generate(mod_, law_, nx, ny, nz, h, plan_, why)) return false;
     if (!device_ready(why)) return false;
     sms_ = sm_count();
@@ -432,13 +453,19 @@ bool Engine::upload(int field, const void* src, bool device, std::string& why)
     if (!cuda_ok(cudaMemcpyAsync(dst, src, cells_ * sizeof(float), kind, stream_), "upload", why)) return false;
     // The bounds of what arrived, for the idle-term test (CudaSolver.cpp:820-920 looks over uploaded planes the same
     // way), taken on the card once the cells are there: one read at HBM rate instead of a host loop over every cell.
+    // The caller's buffer is read only during the call: measure_bounds waits for the copy.
+    return measure_bounds(field, why);
+}
+
+bool Engine::measure_bounds(int field, std::string& why)
+{
+    float* dst = now_[static_cast<std::size_t>(field)];
     FeCheck* rec = bounds_rec_;
-    if (!cuda_ok(cudaMemsetAsync(rec, 0, sizeof(FeCheck), stream_), "upload bounds", why)) return false;
-    if (!cuda_ok(launch_bounds(dst, cells_, rec, sms_, stream_), "upload bounds", why)) return false;
+    if (!cuda_ok(cudaMemsetAsync(rec, 0, sizeof(FeCheck), stream_), "bounds", why)) return false;
+    if (!cuda_ok(launch_bounds(dst, cells_, rec, sms_, stream_), "bounds", why)) return false;
     FeCheck got{};
-    if (!cuda_ok(cudaMemcpyAsync(&got, rec, sizeof(FeCheck), cudaMemcpyDeviceToHost, stream_), "upload bounds", why)) return false;
-    // The caller's buffer is read only during the call: wait for the copy (and the 8 bytes of keys).
-    if (!cuda_ok(cudaStreamSynchronize(stream_), "upload", why)) return false;
+    if (!cuda_ok(cudaMemcpyAsync(&got, rec, sizeof(FeCheck), cudaMemcpyDeviceToHost, stream_), "bounds", why)) return false;
+    if (!cuda_ok(cudaStreamSynchronize(stream_), "bounds", why)) return false;
     Bounds b{};
     const unsigned lo_key = ~got.lo_inv;
     if (got.hi_key != 0u && lo_key != 0xffffffffu) b = Bounds{key_to_float(lo_key), key_to_float(got.hi_key)};
@@ -446,6 +473,84 @@ bool Engine::upload(int field, const void* src, bool device, std::string& why)
     zero_[static_cast<std::size_t>(field)] = (b.lo == 0.0 && b.hi == 0.0) ? 1 : 0;
     carry_[static_cast<std::size_t>(field)] = Carry{};
     return true;
+}
+
+bool Engine::shift(int dx, int dy, int dz, std::string& why)
+{
+    if (!sync(why)) return false;
+    auto wrap = [](int v, int n) { return ((v % n) + n) % n; };
+    dx = wrap(dx, nx_);
+    dy = wrap(dy, ny_);
+    dz = wrap(dz, nz_);
+    if (dx == 0 && dy == 0 && dz == 0) return true;
+    if (rotate_scratch_ == nullptr &&
+        !cuda_ok(cudaMalloc(reinterpret_cast<void**>(&rotate_scratch_), cells_ * sizeof(float)), "cudaMalloc (window)", why)) {
+        return false;
+    }
+    // Every field's cells and every slot (the stages are recomputed, but distance's seeds and poisson's warm start are
+    // kept from step to step and move with the window as a ring's would).
+    std::vector<float*> moving(now_.begin(), now_.end());
+    moving.insert(moving.end(), slot_.begin(), slot_.end());
+    for (float* buf : moving) {
+        if (!cuda_ok(launch_rotate(buf, rotate_scratch_, nx_, ny_, nz_, dx, dy, dz, sms_, stream_), "window", why)) return false;
+        if (!cuda_ok(cudaMemcpyAsync(buf, rotate_scratch_, cells_ * sizeof(float), cudaMemcpyDeviceToDevice, stream_), "window", why)) {
+            return false;
+        }
+    }
+    // The same values, so the same bounds; the totals are summed afresh (in the new cell order).
+    carry_.assign(carry_.size(), Carry{});
+    return cuda_ok(cudaStreamSynchronize(stream_), "window", why);
+}
+
+bool Engine::upload_box(int field, const float* host, const int box[6], std::string& why)
+{
+    if (field < 0 || static_cast<std::size_t>(field) >= now_.size()) {
+        why = "no field " + std::to_string(field);
+        return false;
+    }
+    const int x0 = std::max(0, box[0]), y0 = std::max(0, box[1]), z0 = std::max(0, box[2]);
+    const int x1 = std::min(nx_, box[3]), y1 = std::min(ny_, box[4]), z1 = std::min(nz_, box[5]);
+    if (x0 >= x1 || y0 >= y1 || z0 >= z1) return true;
+    if (!sync(why)) return false;
+    float* dst = now_[static_cast<std::size_t>(field)];
+    const std::size_t pitch = static_cast<std::size_t>(nx_) * sizeof(float);
+    for (int z = z0; z < z1; ++z) {
+        const std::size_t at = (static_cast<std::size_t>(z) * ny_ + y0) * nx_ + x0;
+        if (!cuda_ok(cudaMemcpy2DAsync(dst + at, pitch, host + at, pitch, static_cast<std::size_t>(x1 - x0) * sizeof(float),
+                         static_cast<std::size_t>(y1 - y0), cudaMemcpyHostToDevice, stream_),
+                "upload box", why)) {
+            return false;
+        }
+    }
+    return measure_bounds(field, why);
+}
+
+bool Engine::upload_planes(int field, const float* host, const unsigned char* planes, std::string& why)
+{
+    if (field < 0 || static_cast<std::size_t>(field) >= now_.size()) {
+        why = "no field " + std::to_string(field);
+        return false;
+    }
+    if (!sync(why)) return false;
+    float* dst = now_[static_cast<std::size_t>(field)];
+    const std::size_t plane = static_cast<std::size_t>(nx_) * ny_;
+    bool any = false;
+    for (int z = 0; z < nz_;) {
+        if (!planes[z]) {
+            ++z;
+            continue;
+        }
+        int end = z + 1;
+        while (end < nz_ && planes[end]) ++end;
+        // A run of flagged planes is one contiguous copy.
+        if (!cuda_ok(cudaMemcpyAsync(dst + plane * z, host + plane * z, plane * (end - z) * sizeof(float), cudaMemcpyHostToDevice, stream_),
+                "upload planes", why)) {
+            return false;
+        }
+        any = true;
+        z = end;
+    }
+    return !any || measure_bounds(field, why);
 }
 
 void Engine::mark_halo(int field)

@@ -64,9 +64,19 @@ class Engine {
 public:
     ~Engine();
     bool create(const std::vector<law::Source>& sources, int nx, int ny, int nz, double h, std::string& why);
+    // From a law already compiled and lowered (a law given as its IR).
+    bool create(law::Law law, ir::Module module, int nx, int ny, int nz, double h, std::string& why);
 
     // Host <-> card.
     bool upload(int field, const void* src, bool device, std::string& why);
+    // The lattice's window moved by (dx, dy, dz) cells: the cell now at c holds what was at c + d (FieldEdits::shift,
+    // src/field/Backend.hpp:31-39). Every field and per-cell slot is carried over, the cells that left wrapping round
+    // to the arriving side, as a ring-addressed lattice would read them; the caller then uploads the arriving boxes.
+    bool shift(int dx, int dy, int dz, std::string& why);
+    // Uploads only the cells of a box [x0, x1) x [y0, y1) x [z0, z1), or only the flagged z-planes, from a host array
+    // of the whole field (the reference's host FieldSet is the truth between steps; CudaSolver.cpp:779-920).
+    bool upload_box(int field, const float* host, const int box[6], std::string& why);
+    bool upload_planes(int field, const float* host, const unsigned char* planes, std::string& why);
     // A field's cells were changed in place on the device by someone else (ordered on the engine's stream): what the
     // engine knew of its bounds no longer holds.
     void mark_edited(int field);
@@ -173,6 +183,8 @@ private:
     unsigned* counts_ = nullptr; // FE_MAX_OUT counters, then the error word
     unsigned* flags_ = nullptr;  // change flags of the distance and poisson ops
     FeCheck* bounds_rec_ = nullptr; // the bounds of an upload (lo_inv / hi_key keys)
+    float* rotate_scratch_ = nullptr; // one field's cells, for moving the window (allocated at the first shift)
+    bool measure_bounds(int field, std::string& why); // the field's exact bounds, taken on the card
     std::vector<PendingStep> pending_;
     std::vector<double> param_host_;
     bool params_dirty_ = true;

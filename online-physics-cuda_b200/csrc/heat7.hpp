@@ -44,6 +44,8 @@ constexpr int kTotalsBlocks = 1184;
 cudaError_t launch_totals(const float* v, size_t n, FeCheck* rec, double* partials, unsigned* count, cudaStream_t stream);
 // The least and largest non-NaN value of n cells into rec->lo_inv / hi_key (ordered keys; rec all zero before).
 cudaError_t launch_bounds(const float* v, size_t n, FeCheck* rec, int sms, cudaStream_t stream);
+// dst = src with its window moved by (dx, dy, dz), 0 <= d < n on each axis, wrapping (totals.cu rotate_f32).
+cudaError_t launch_rotate(const float* src, float* dst, int nx, int ny, int nz, int dx, int dy, int dz, int sms, cudaStream_t stream);
 cudaError_t launch_copy(const float* a, float* b, size_t n, int sms, cudaStream_t stream);
 // The solves of distance and poisson (field_solves.cu), after their seed pass; each kernel returns at once unless *flag.
 // distance slots: 0 the answer, 1 seeds inside, 2 seeds outside, 3 and 4 scratch, 5 and 6 squared distances. Launches:

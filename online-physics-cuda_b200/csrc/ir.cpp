@@ -494,10 +494,11 @@ void program_json(Json& j, const Program& p)
 
 } // namespace
 
-Module lower(const law::Law& law)
+Module lower(const law::Law& law, int prelower)
 {
     Module m;
     Builder b(m, law);
+    for (int n = 0; n < prelower; ++n) b.value_of(n);
     for (const law::Term& term : law.terms) {
         m.terms.push_back(start_program(b, term.name, term.equations, term.max_dt));
         m.terms.back().conserves = term.conserves;

@@ -71,7 +71,8 @@ struct Module {
 
 constexpr int kInlineBudget = 48;
 
-Module lower(const law::Law& law);
+// `prelower`: nodes [0, prelower) are lowered first, in order (a law rebuilt from IR instructions keeps their ids).
+Module lower(const law::Law& law, int prelower = 0);
 // The code generator's own staging on top of the IR's (the IR, and its JSON, stay the reference's): a value that
 // stencil ops read at several offsets, each read inlining its whole expression, is stored once when its inlined cost
 // times the points read passes the inline budget (the IR's rule counts one reader at a time). Stored or inlined it is

@@ -94,6 +94,31 @@ cudaError_t launch_bounds(const float* v, size_t n, FeCheck* rec, int sms, cudaS
     return cudaGetLastError();
 }
 
+// dst(x, y, z) = src((x + dx) mod nx, (y + dy) mod ny, (z + dz) mod nz): a lattice whose window moved by (dx, dy, dz)
+// cells, every cell's value carried to where it now is and the cells that left wrapped round to the side that arrives
+// (what a ring-addressed lattice reads there after its origin moves). 0 <= dx < nx, 0 <= dy < ny, 0 <= dz < nz.
+__global__ void __launch_bounds__(256) rotate_f32(const float* __restrict__ src, float* __restrict__ dst, int nx, int ny, int nz, int dx,
+    int dy, int dz)
+{
+    const size_t n = static_cast<size_t>(nx) * ny * nz;
+    for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(i % nx);
+        const size_t row = i / nx;
+        const int y = static_cast<int>(row % ny);
+        const int z = static_cast<int>(row / ny);
+        const int sx = x + dx >= nx ? x + dx - nx : x + dx;
+        const int sy = y + dy >= ny ? y + dy - ny : y + dy;
+        const int sz = z + dz >= nz ? z + dz - nz : z + dz;
+        dst[i] = src[(static_cast<size_t>(sz) * ny + sy) * nx + sx];
+    }
+}
+
+cudaError_t launch_rotate(const float* src, float* dst, int nx, int ny, int nz, int dx, int dy, int dz, int sms, cudaStream_t stream)
+{
+    rotate_f32<<<8 * sms, 256, 0, stream>>>(src, dst, nx, ny, nz, dx, dy, dz);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_totals(const float* v, size_t n, FeCheck* rec, double* partials, unsigned* count, cudaStream_t stream)
 {
     totals_f32<<<kTotalsBlocks, 256, 0, stream>>>(v, n, rec, partials, count);

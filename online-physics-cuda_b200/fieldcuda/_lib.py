@@ -119,6 +119,12 @@ SIGNATURES = {
                                          _c.c_void_p]),
     "fe_law_create": (_i, [_cs, _cs, _i, _i, _i, _d, _c.POINTER(_p)]),
     "fe_law_destroy": (None, [_p]),
+    "fe_law_create_ir": (_i, [_cs, _i, _i, _i, _d, _c.POINTER(_p)]),
+    "fe_law_ir_check": (_i, [_cs, _p, _s, _c.POINTER(_s)]),
+    "fe_law_source_ir": (_i, [_cs, _i, _i, _i, _d, _p, _s, _c.POINTER(_s)]),
+    "fe_law_shift": (_i, [_p, _i, _i, _i]),
+    "fe_law_upload_box": (_i, [_p, _i, _p, _i, _i, _i, _i, _i, _i]),
+    "fe_law_upload_planes": (_i, [_p, _i, _p, _p]),
     "fe_law_ir_json": (_i, [_cs, _p, _s, _c.POINTER(_s)]),
     "fe_law_ir_listing": (_i, [_cs, _p, _s, _c.POINTER(_s)]),
     "fe_law_adjoint": (_i, [_cs, _cs, _p, _s, _c.POINTER(_s)]),

@@ -31,8 +31,9 @@ def test_reference_bench_laws_lower_identically():
     law lower to the same IR as its lawc prints."""
     import subprocess
     lawc = os.path.join(ROOT, "oracle", "_ref", "lawc")
-    ref_root = "/root/reference"
-    if not (os.path.exists(lawc) and os.path.isdir(ref_root)):
+    where = os.path.join(ROOT, "oracle", "_ref", "REFERENCE")  # the checkout oracle/Makefile built lawc from
+    ref_root = open(where).read().strip() if os.path.exists(where) else ""
+    if not (os.path.exists(lawc) and ref_root and os.path.isdir(ref_root)):
         pytest.skip("the reference's sources and lawc are not here")
     from fieldcuda import solver
     sets = [[p] for p in sorted(glob.glob(os.path.join(ref_root, "bench", "laws", "*.law")))]
@@ -45,6 +46,45 @@ def test_reference_bench_laws_lower_identically():
             n["loaded"] = False
         mine = json.loads(solver.ir_json("".join(open(p).read() + "\n" for p in paths)))
         assert mine == ref, paths
+        # The same IR taken in as IR (fe_law_create_ir's ingest) is the same law.
+        assert ir_check(json.dumps(ref)) == ref, paths
+
+
+IRS = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "ir", "*.json")))
+
+
+def ir_check(text):
+    import ctypes
+    from fieldcuda import _lib
+    lib = _lib.lib()
+    need = ctypes.c_size_t()
+    _lib.check(lib.fe_law_ir_check(text.encode(), None, 0, ctypes.byref(need)))
+    buf = ctypes.create_string_buffer(need.value)
+    _lib.check(lib.fe_law_ir_check(text.encode(), buf, need.value, ctypes.byref(need)))
+    return json.loads(buf.value.decode())
+
+
+@pytest.mark.parametrize("path", IRS, ids=lambda p: os.path.basename(p))
+def test_law_given_as_the_references_ir_is_the_same_law(path, monkeypatch):
+    """fe_law_create_ir's ingest: the reference's IR JSON (made by its lawc) rebuilt into a law and lowered again gives
+    that JSON back, instruction for instruction (folded-away numbers included) and program for program."""
+    monkeypatch.chdir(ROOT)  # net weight files named in the IR are repository paths
+    text = open(path).read()
+    assert ir_check(text) == json.loads(text)
+
+
+def test_ir_ingest_refuses_what_it_cannot_take():
+    from fieldcuda import _lib
+    text = open(os.path.join(ROOT, "tests", "golden", "ir", "heat.json")).read()
+    for bad in ("{", "[]", text.replace('"version":1', '"version":2'), text.replace('"op":"diffuse"', '"op":"sprinkle"')):
+        with pytest.raises(_lib.FeError) as e:
+            ir_check(bad)
+        assert e.value.code == _lib.FE_ELAW
+    # An edited program (its stage list) no longer matches what its instructions lower to.
+    doc = json.loads(open(os.path.join(ROOT, "tests", "golden", "ir", "heston_douglas.json")).read())
+    doc["terms"][0]["stages"] = doc["terms"][0]["stages"][:-1]
+    with pytest.raises(_lib.FeError, match="does not lower back"):
+        ir_check(json.dumps(doc))
 
 
 def test_law_errors_match_the_reference_word_for_word():
