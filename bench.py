@@ -422,6 +422,33 @@ def c2_section(stream_sync, peak, cpu=True):
     return out
 
 
+def cpu_reference_run(law_path, grid, dt, steps, fields):
+    """The reference's own OpenMP CPU solver (oracle/_ref/lawc) on a law file: ms a step over `steps` after one warm-up
+    step, all host cores. grid = (nx, ny, nz, h); fields: name -> (nz, ny, nx) float32 starting values. None without
+    lawc."""
+    lawc = os.path.join(ROOT, "oracle", "_ref", "lawc")
+    if not os.path.exists(lawc):
+        return None
+    import numpy as np
+    threads = os.cpu_count() or 1
+    nx, ny, nz, h = grid
+    work = tempfile.mkdtemp(prefix="fe_cpu_")
+    try:
+        scene = os.path.join(work, "s.scene")
+        open(scene, "w").write(f"grid {nx} {ny} {nz} {h!r}\nlaw {law_path}\n")
+        init = os.path.join(work, "init")
+        os.makedirs(init)
+        for k, v in fields.items():
+            np.ascontiguousarray(v, np.float32).tofile(os.path.join(init, k + ".bin"))
+        out = os.path.join(work, "t.json")
+        subprocess.run([lawc, "--scene", scene, "--init", init, "--steps", str(steps + 1), "--dt", repr(dt), "--json", out,
+                        "--warmup", "1"], check=True, env=dict(os.environ, OMP_NUM_THREADS=str(threads)),
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        return json.load(open(out))["mean_ms"], threads
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
+
+
 def cpu_reference_law(text, n, dt, steps, fields):
     """Times the reference's own OpenMP CPU solver (oracle/_ref/lawc) on law `text` at n^3: ms/step over `steps` after
     one warm-up, all host cores. `fields`: name -> ("uniform", seed) starting states, U[-1, 1]. None without lawc."""
@@ -449,21 +476,65 @@ def cpu_reference_law(text, n, dt, steps, fields):
         shutil.rmtree(work, ignore_errors=True)
 
 
-HESTON_EXPLICIT_LAW = os.path.join(ROOT, "tests", "laws", "heston_explicit.law")
+HESTON_EXPLICIT_T_LAW = os.path.join(ROOT, "tests", "laws", "heston_explicit_T.law")
+HESTON_DOUGLAS_LAW = os.path.join(ROOT, "tests", "laws", "heston_douglas.law")
 HESTON_CF = os.path.join(ROOT, "tests", "golden", "heston", "cf_2048.npz")
 HESTON_BUCKETS = ((128, 64), (256, 128), (512, 256))
+
+
+def err_stats(e):
+    import numpy as np
+    e = np.asarray(e, np.float64)
+    return {"options": int(e.size), "rms": float(np.sqrt(np.mean(e * e))), "median": float(np.median(e)),
+            "p90": float(np.percentile(e, 90)), "max": float(e.max())}
+
+
+def plain_heston_bucket(opts, nx, ny, stream_sync, planes=None):
+    """The plain method on one bucket: explicit Euler (tests/laws/heston_explicit_T.law: heston_explicit.law's operator
+    with each option's time to maturity scaled onto s in [0, 1]) through fe_law_step, the bucket's options (or the
+    first `planes` of them) as the z-planes of one lattice, stepped at the law's stability limit to s = 1. Returns
+    (device ms, substeps, prices)."""
+    import numpy as np
+    import torch
+    from fieldcuda.heston import lattice_fields, price_at
+    from fieldcuda.solver import Solver
+    group = opts if planes is None else opts[:planes]
+    fields, h = lattice_fields(group, nx, ny)
+    fields["mat"] = np.broadcast_to(np.array([o["maturity"] for o in group], np.float32)[:, None, None],
+                                    fields["V"].shape).copy()
+    s = Solver(open(HESTON_EXPLICIT_T_LAW).read(), nx, ny, len(group), h, "heston_explicit_T.law")
+    for k, v in fields.items():
+        s.set_field(k, v)
+    # ds = 1 in chunks the substep cap (4096 a step) allows: the limit is 0.25 h^2 / max(T (var + sig_v h / 2)).
+    limit = min(0.25 * h * h / (o["maturity"] * o["sigma"] * ny * h) for o in group)
+    chunks = int(np.ceil(1.0 / limit / 4000.0))
+    st = torch.cuda.ExternalStream(s.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream_sync()
+    e0.record(st)
+    substeps = 0
+    for _ in range(chunks):
+        s.step(1.0 / chunks)
+        substeps += s.last_substeps()[0]
+    e1.record(st)
+    st.synchronize()
+    ms = e0.elapsed_time(e1)
+    V = s.values("V")
+    s.close()
+    return ms, substeps, np.array([price_at(V[z], o) for z, o in enumerate(group)])
 
 
 def heston_batch_section(stream_sync):
     """Batched Heston ADI (Douglas, theta = 1/2): 2048 seeded options on their own grids (128 x 64, 256 x 128 or 512 x
     256), 512 steps, priced in one persistent launch (autotuned, CUDA-graph replayed), against the plain method at the
-    same grids: the explicit law (tests/laws/heston_explicit.law, the same operator, stepped at its stability limit)
-    through the law backend, the reference's way of batching (every bucket's options as the z-planes of one lattice).
-    Errors are against FP64 characteristic-function prices of the same options (tests/golden/heston/cf_2048.npz)."""
+    same grids: explicit Euler (the same operator, tests/laws/heston_explicit_T.law, each option's maturity scaled onto
+    one time axis) through the law backend, every bucket's options as the z-planes of one lattice, the reference's way
+    of batching. The two smaller buckets run end to end, every option priced by both methods; the 512 x 256 bucket's
+    plain time is extrapolated from 128 of its options over 2000 substeps (labelled). Errors are against FP64
+    characteristic-function prices of the same options (tests/golden/heston/cf_2048.npz), by bucket and by Feller ratio
+    2 kappa theta / sigma^2. The reference's own OpenMP solver is timed on a sample of the 256 x 128 bucket."""
     import numpy as np
-    import torch
-    from fieldcuda.heston import DOUGLAS, HestonBatch, lattice_fields, price_at, sample_options
-    from fieldcuda.solver import Solver
+    from fieldcuda.heston import DOUGLAS, HestonBatch, sample_options
 
     n, steps = 2048, 512
     opts = sample_options(n, 1)
@@ -482,70 +553,130 @@ def heston_batch_section(stream_sync):
     cells = sum(o["nx"] * o["ny"] for o in opts)
     out = {"options": n, "steps": steps, "scheme": "Douglas (theta = 1/2)", "ms": ms, "options_per_s": n / (ms * 1e-3),
            "cell_steps_per_s": cells * steps / (ms * 1e-3), "split": {"mx": split[0], "sy": split[1], "threads": split[2]},
-           "clusters": clusters, "tasks": tasks,
+           "clusters": clusters, "tasks": tasks, "readout": "bicubic (4 x 4 cell centres, local Lagrange) at (ln S0, v0)",
            "hbm_bytes": 8 * cells, "hbm_note": "each option's state stays in shared memory for all its steps: 8 B a cell a run"}
+    buckets = {f"{nx}x{ny}": [i for i, o in enumerate(opts) if (o["nx"], o["ny"]) == (nx, ny)] for nx, ny in HESTON_BUCKETS}
     if cf is not None:
         err = np.abs(prices - cf)
-        out["error_vs_cf"] = {"median": float(np.median(err)), "p90": float(np.percentile(err, 90)), "max": float(err.max())}
+        feller = np.array([2 * o["kappa"] * o["theta"] / o["sigma"] ** 2 for o in opts])
+        out["error_vs_cf"] = err_stats(err)
+        out["error_vs_cf_by_bucket"] = {k: err_stats(err[idx]) for k, idx in buckets.items()}
+        bins = ((0, 0.25), (0.25, 0.5), (0.5, 1.0), (1.0, 1e9))
+        out["error_vs_cf_by_feller_ratio"] = {f"[{a}, {b})": err_stats(err[(feller >= a) & (feller < b)])
+                                              for a, b in bins if np.any((feller >= a) & (feller < b))}
+        below = np.array([o["v0"] < 0.5 * o["sigma"] * 6.0 / o["nx"] for o in opts])
+        out["error_vs_cf_v0_below_first_row"] = err_stats(err[below]) if below.any() else None
+        worst = np.argsort(err)[-5:][::-1]
+        out["worst_options"] = [dict(err=float(err[i]), price=float(prices[i]), cf=float(cf[i]), feller=float(feller[i]),
+                                     **{k: opts[i][k] for k in ("nx", "ny", "strike", "maturity", "v0", "kappa", "theta",
+                                                                "sigma", "rho", "r")}) for i in worst]
 
-    # The plain method: explicit Euler on each bucket's lattice at its stability limit. Its cost is measured per
-    # substep on up to 128 planes of the bucket and scaled by planes and by the substeps that reach each bucket's
-    # longest maturity (the explicit pass streams the lattice from HBM, so its time grows with the planes).
-    law = open(HESTON_EXPLICIT_LAW).read()
-    plain_ms = 0.0
+    # The plain method, end to end on the two smaller buckets (every option priced), extrapolated on the largest.
     plain = {}
-    sample_err = {"adi": [], "plain": []}
+    measured_idx = []
+    plain_ms_measured = 0.0
     for nx, ny in HESTON_BUCKETS:
-        group = [i for i, o in enumerate(opts) if (o["nx"], o["ny"]) == (nx, ny)]
-        if not group:
-            continue
-        planes = [opts[i] for i in group[:128]]
-        fields, h = lattice_fields(planes, nx, ny)
-        s = Solver(law, nx, ny, len(planes), h, "heston_explicit.law")
-        for k, v in fields.items():
-            s.set_field(k, v)
-        max_dt = 0.25 * h / (max(o["sigma"] for o in planes) * ny)   # the law's limit: 0.25 h^2 / (sig_v h ny)
-        sub = 64
-        s.step(sub * max_dt * 0.999)
-        st = torch.cuda.ExternalStream(s.stream)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        stream_sync()
-        e0.record(st)
-        s.step(sub * max_dt * 0.999)
-        e1.record(st)
-        st.synchronize()
-        per_sub = e0.elapsed_time(e1) / max(1, max(s.last_substeps()))
-        s.close()
-        t_max = max(opts[i]["maturity"] for i in group)
-        sig_max = max(opts[i]["sigma"] for i in group)
-        subs = int(np.ceil(t_max / (0.25 * h / (sig_max * ny))))
-        bucket_ms = per_sub * (len(group) / len(planes)) * subs
-        plain_ms += bucket_ms
-        plain[f"{nx}x{ny}"] = {"options": len(group), "substeps": subs, "ms_per_substep_128_planes": per_sub, "ms": bucket_ms}
-        # Equal error: two options of the bucket priced by the plain method to maturity (each alone), beside the batch.
-        if cf is not None:
-            for i in group[:2]:
-                o = opts[i]
-                f1, _ = lattice_fields([o], nx, ny)
-                s1 = Solver(law, nx, ny, 1, h, "heston_explicit.law")
-                for k, v in f1.items():
-                    s1.set_field(k, v)
-                lim = 0.25 * h / (o["sigma"] * ny)
-                nsteps = int(np.ceil(o["maturity"] / (4000 * lim)))
-                for _ in range(nsteps):
-                    s1.step(o["maturity"] / nsteps)
-                p = price_at(s1.values("V")[0], o)
-                s1.close()
-                sample_err["plain"].append(abs(p - cf[i]))
-                sample_err["adi"].append(float(abs(prices[i] - cf[i])))
-    out["plain"] = {"method": "explicit Euler law (tests/laws/heston_explicit.law) through fe_law_step, same grids",
+        key = f"{nx}x{ny}"
+        idx = buckets[key]
+        group = [opts[i] for i in idx]
+        if (nx, ny) != HESTON_BUCKETS[-1]:
+            pms, subs, pp = plain_heston_bucket(group, nx, ny, stream_sync)
+            row = {"options": len(idx), "substeps": subs, "ms": pms, "measured": True}
+            if cf is not None:
+                pe = np.abs(pp - cf[idx])
+                ae = np.abs(prices[idx] - cf[idx])
+                row["plain_error_vs_cf"] = err_stats(pe)
+                row["adi_error_vs_cf"] = err_stats(ae)
+                row["adi_within_plain_error_1e_3"] = float(np.mean(ae <= pe + 1e-3))
+                row["max_abs_adi_minus_plain"] = float(np.abs(prices[idx] - pp).max())
+            plain_ms_measured += pms
+            measured_idx += idx
+        else:
+            # 128 of its options over 2000 substeps, scaled by options and by the substeps its longest option needs.
+            sample = group[:128]
+            limit = min(0.25 * (6.0 / nx) ** 2 / (o["maturity"] * o["sigma"] * ny * (6.0 / nx)) for o in group)
+            subs = int(np.ceil(1.0 / limit))
+            pms, psub, _ = plain_heston_bucket_sample(sample, nx, ny, stream_sync, 2000)
+            row = {"options": len(idx), "substeps": subs, "ms": pms / psub * subs * len(group) / len(sample),
+                   "measured": False, "extrapolated_from": f"{len(sample)} options x {psub} substeps in {pms:.1f} ms"}
+        plain[key] = row
+    plain_ms = sum(r["ms"] for r in plain.values())
+    out["plain"] = {"method": "explicit Euler law (tests/laws/heston_explicit_T.law) through fe_law_step, same grids",
                     "ms": plain_ms, "options_per_s": n / (plain_ms * 1e-3), "buckets": plain}
-    if sample_err["plain"]:
-        out["equal_error_sample"] = {"options": len(sample_err["plain"]),
-                                     "adi_abs_err": [round(v, 6) for v in sample_err["adi"]],
-                                     "plain_abs_err": [round(v, 6) for v in sample_err["plain"]]}
     out["speedup_vs_plain"] = plain_ms / ms
+    # A fully measured ratio: the ADI batch of just the measured buckets' options against their plain runs.
+    with HestonBatch([opts[i] for i in measured_idx], steps, DOUGLAS) as b2:
+        b2.autotune()
+        b2.run(use_graph=True)
+        ms2 = statistics.median([b2.time(use_graph=True) for _ in range(3)])
+    out["measured_buckets"] = {"options": len(measured_idx), "adi_ms": ms2, "plain_ms": plain_ms_measured,
+                               "speedup": plain_ms_measured / ms2}
+    cpu = cpu_reference_heston(256, 128, [opts[i] for i in buckets["256x128"][:16]], 4)
+    if cpu is not None:
+        ms_step, cores = cpu
+        per_option = ms_step / 16 * steps
+        out["cpu_baseline"] = {"value": 1e3 / per_option, "unit": "options/s", "cores": cores, "kind": "reference",
+                               "sample": "the reference's lawc on tests/laws/heston_douglas.law, 16 options of the 256 x 128 "
+                                         f"bucket as z-planes, 4 timed steps after 1 warm-up ({ms_step:.1f} ms a step), "
+                                         f"scaled to {steps} steps an option"}
     return out
+
+
+def plain_heston_bucket_sample(group, nx, ny, stream_sync, substeps):
+    """Device time of `substeps` explicit substeps (heston_explicit_T.law) on these options as the planes of one lattice."""
+    import numpy as np
+    import torch
+    from fieldcuda.heston import lattice_fields
+    from fieldcuda.solver import Solver
+    fields, h = lattice_fields(group, nx, ny)
+    fields["mat"] = np.broadcast_to(np.array([o["maturity"] for o in group], np.float32)[:, None, None],
+                                    fields["V"].shape).copy()
+    s = Solver(open(HESTON_EXPLICIT_T_LAW).read(), nx, ny, len(group), h, "heston_explicit_T.law")
+    for k, v in fields.items():
+        s.set_field(k, v)
+    limit = min(0.25 * h * h / (o["maturity"] * o["sigma"] * ny * h) for o in group)
+    s.step(0.999 * limit * 8)  # warm-up: compile and a few substeps
+    st = torch.cuda.ExternalStream(s.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    done = 0
+    stream_sync()
+    e0.record(st)
+    while done < substeps:
+        s.step(0.999 * limit * 1000)
+        done += s.last_substeps()[0]
+    e1.record(st)
+    st.synchronize()
+    ms = e0.elapsed_time(e1)
+    s.close()
+    return ms, done, None
+
+
+def cpu_reference_heston(nx, ny, group, steps):
+    """The reference's OpenMP solver (oracle/_ref/lawc) on tests/laws/heston_douglas.law with these options as z-planes:
+    ms a step (after one warm-up step), all host cores; None without lawc."""
+    lawc = os.path.join(ROOT, "oracle", "_ref", "lawc")
+    if not os.path.exists(lawc):
+        return None
+    import numpy as np
+    from fieldcuda.heston import lattice_fields
+    threads = os.cpu_count() or 1
+    fields, h = lattice_fields(group, nx, ny)
+    work = tempfile.mkdtemp(prefix="fe_cpu_")
+    try:
+        scene = os.path.join(work, "s.scene")
+        open(scene, "w").write(f"grid {nx} {ny} {len(group)} {h!r}\nlaw {HESTON_DOUGLAS_LAW}\n")
+        init = os.path.join(work, "init")
+        os.makedirs(init)
+        for k, v in fields.items():
+            np.ascontiguousarray(v, np.float32).tofile(os.path.join(init, k + ".bin"))
+        out = os.path.join(work, "t.json")
+        dt = min(o["maturity"] for o in group) / 512
+        subprocess.run([lawc, "--scene", scene, "--init", init, "--steps", str(steps + 1), "--dt", repr(dt), "--json", out,
+                        "--warmup", "1"], check=True, env=dict(os.environ, OMP_NUM_THREADS=str(threads)),
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        return json.load(open(out))["mean_ms"], threads
+    finally:
+        shutil.rmtree(work, ignore_errors=True)
 
 
 def multifield_section(n, steps, warmup, stream_sync):
@@ -641,7 +772,6 @@ def nets_section(stream_sync):
     return {"cells": n * n * nz, "dt": dt, "laws": out}
 
 
-HESTON_DOUGLAS_LAW = os.path.join(ROOT, "tests", "laws", "heston_douglas.law")
 HESTON_CALIB = os.path.join(ROOT, "tests", "golden", "heston", "calib_512.npz")
 
 
@@ -676,7 +806,27 @@ def calibration_section():
         fd.append((cal.loss_only(xp) - cal.loss_only(xm)) / (2 * e))
     cal.close()
     fd = np.array(fd)
+    out_cpu = None
+    # The reference cannot differentiate through its tridiagonal solves: its way to this gradient is central
+    # differences of its CPU forward (10 losses). Timed on a sample (64 of the 512 options, 4 Douglas steps) and
+    # scaled to the whole calibration lattice, its 512 steps and the 11 losses (the base and 10 perturbed).
+    from fieldcuda.heston import lattice_fields
+    sample = [dict(nx=nx, ny=ny, strike=float(k), maturity=common["maturity"], spot=common["spot"], v0=truth["v0"],
+                   kappa=truth["kappa"], theta=truth["theta"], sigma=truth["sigma"], rho=truth["rho"], r=common["r"])
+              for k in strikes[:64]]
+    fields, h = lattice_fields(sample, nx, ny)
+    res = cpu_reference_run(HESTON_DOUGLAS_LAW, (nx, ny, 64, h), common["maturity"] / steps, 4, fields)
+    if res is not None:
+        ms_step, cores = res
+        est_ms = ms_step * (512 / 64) * steps * 11
+        out_cpu = {"value": 1e3 / est_ms, "unit": "gradients/s", "cores": cores, "kind": "reference",
+                   "sample": f"the reference's lawc on tests/laws/heston_douglas.law, 64 of the options as z-planes of "
+                             f"{nx} x {ny}, 4 timed steps after 1 warm-up ({ms_step:.1f} ms a step), scaled to 512 options, "
+                             f"{steps} steps and 11 losses (central differences of the 5 parameters)",
+                   "estimated_ms_a_gradient": est_ms}
     return {"options": 512, "lattice": f"{nx} x {ny} x 512 planes", "steps": steps,
+            "gradients_per_s": 1e3 / ms_grad, "cpu_baseline": out_cpu,
+            "speedup_vs_cpu": (out_cpu["estimated_ms_a_gradient"] / ms_grad) if out_cpu else None,
             "checkpoints": int(np.ceil(np.sqrt(steps))), "loss": loss,
             "gradient": dict(zip(Calibration.NAMES, map(float, grad))), "central_fd": dict(zip(Calibration.NAMES, map(float, fd))),
             "fd_rel_err": dict(zip(Calibration.NAMES, map(float, np.abs(grad - fd) / np.maximum(np.abs(fd), 1e-12)))),
@@ -764,10 +914,21 @@ def fhn_learned_section(samples=1000, frames=100, train_samples=64, iters=3000):
                 e64.append(float((((a[:4].cpu().numpy() - ref[0]) ** 2 + (b[:4].cpu().numpy() - ref[1]) ** 2) / 2).mean()))
             out[name]["rmse_vs_fp64_4_seeds"] = float(np.sqrt(np.mean(e64)))
     corr.close()
+    # The reference's own OpenMP solver on the plain 128 x 128 law (the judge), 16 samples as z-planes over 2 frames,
+    # scaled to solves (100 frames) a second.
+    cu, cv = fhn_initial(list(range(2000, 2016)), 128)
+    res = cpu_reference_run(FHN_LAW, (128, 128, 16, 2.0 / 128), 0.05, 2, {"u": cu, "v": cv})
+    cpu = None
+    if res is not None:
+        ms_frame, cores = res
+        cpu = {"value": 16 / (ms_frame * frames * 1e-3), "unit": "solves/s", "cores": cores, "kind": "reference",
+               "sample": f"the reference's lawc on tests/laws/fhn_rk4.law, 128 x 128 x 16 samples, 2 timed frames of 0.05 "
+                         f"after 1 warm-up ({ms_frame:.1f} ms a frame), scaled to {frames} frames a solve"}
     learned_err = out["learned_32"]["rmse_vs_plain_128"]
     matches = [m for m in ("plain_32", "plain_64", "plain_128") if out[m]["rmse_vs_plain_128"] <= learned_err]
     equal = matches[0] if matches else None
-    return {"samples": samples, "frames": frames, "methods": out,
+    return {"samples": samples, "frames": frames, "methods": out, "cpu_baseline": cpu,
+            "speedup_learned_vs_cpu_plain_128": (out["learned_32"]["solves_per_s"] / cpu["value"]) if cpu else None,
             "training": {"seeds": train_samples, "pairs": frames, "adam_steps": iters * 3, "rounds": "teacher forcing, then 2 rounds on "
                          "the learned solver's own rollouts", "seconds": train_s, "data_seconds": data_s,
                          "rollout_rmse_train": train_rmse, "plain_rollout_rmse_train": train_plain_rmse},

@@ -610,7 +610,27 @@ __global__ void heston_init(const OptionDev* opts, const float* strikes, int n, 
     }
 }
 
-// Price at (ln S0, v0): bilinear between the four cell centres around it.
+// Weights of the cubic through four consecutive cell centres (at -1, 0, 1, 2 from the second), at offset t from the
+// second: Lagrange interpolation, extrapolating smoothly for t < 0 at the lattice's edge.
+__device__ void cubic_weights(double t, double w[4])
+{
+    w[0] = -t * (t - 1.0) * (t - 2.0) / 6.0;
+    w[1] = (t + 1.0) * (t - 1.0) * (t - 2.0) / 2.0;
+    w[2] = -(t + 1.0) * t * (t - 2.0) / 2.0;
+    w[3] = (t + 1.0) * t * (t - 1.0) / 6.0;
+}
+
+// The first of the four centres along an axis of n cells for a point at fractional centre index f, and the point's
+// offset from the second. f below the first centre (v0 under the first variance row) extrapolates from the edge.
+__device__ int cubic_start(double f, int n, double& t)
+{
+    const int s = max(0, min(n - 4, static_cast<int>(std::floor(f)) - 1));
+    t = f - (s + 1);
+    return s;
+}
+
+// Price at (ln S0, v0): bicubic through the 4 x 4 cell centres around it (local Lagrange, O(h^4) for smooth prices),
+// the way the reference reads its batch (a bicubic spline at (ln 100, v0), bench/finance.py:280-286).
 __global__ void heston_price(const OptionDev* opts, const float* spot, const float* v0, int n, const float* V, float* out)
 {
     const int o = blockIdx.x * blockDim.x + threadIdx.x;
@@ -619,11 +639,18 @@ __global__ void heston_price(const OptionDev* opts, const float* spot, const flo
     const float* U = V + op.at;
     const double fx = (std::log(static_cast<double>(spot[o])) - (op.x0)) / op.h;
     const double fy = static_cast<double>(v0[o]) / (static_cast<double>(op.sigma) * op.h) - 0.5;
-    const int i0 = max(0, min(op.nx - 2, static_cast<int>(std::floor(fx))));
-    const int j0 = max(0, min(op.ny - 2, static_cast<int>(std::floor(fy))));
-    const double tx = fmin(fmax(fx - i0, 0.0), 1.0), ty = fmin(fmax(fy - j0, 0.0), 1.0);
-    const double a = U[j0 * op.nx + i0], b = U[j0 * op.nx + i0 + 1], c = U[(j0 + 1) * op.nx + i0], d = U[(j0 + 1) * op.nx + i0 + 1];
-    out[o] = static_cast<float>((1 - ty) * ((1 - tx) * a + tx * b) + ty * ((1 - tx) * c + tx * d));
+    double tx = 0.0, ty = 0.0, wx[4], wy[4];
+    const int i0 = cubic_start(fx, op.nx, tx);
+    const int j0 = cubic_start(fy, op.ny, ty);
+    cubic_weights(tx, wx);
+    cubic_weights(ty, wy);
+    double p = 0.0;
+    for (int b = 0; b < 4; ++b) {
+        double row = 0.0;
+        for (int a = 0; a < 4; ++a) row += wx[a] * static_cast<double>(U[(j0 + b) * op.nx + i0 + a]);
+        p += wy[b] * row;
+    }
+    out[o] = static_cast<float>(p);
 }
 
 } // namespace

@@ -140,19 +140,27 @@ def lattice_fields(options, nx, ny):
     return out, h
 
 
+def _cubic(f, n):
+    """First of the four cell centres of a cubic read at fractional centre index f on an axis of n, and the Lagrange
+    weights at f (offsets -1, 0, 1, 2 from the second centre; below the first centre it extrapolates)."""
+    s = int(max(0, min(n - 4, np.floor(f) - 1)))
+    t = f - (s + 1)
+    return s, np.array([-t * (t - 1) * (t - 2) / 6, (t + 1) * (t - 1) * (t - 2) / 2, -(t + 1) * t * (t - 2) / 2,
+                        (t + 1) * t * (t - 1) / 6])
+
+
 def price_at(grid, option):
-    """Bilinear price at (ln spot, v0) between the cell centres of one option's (ny, nx) grid, as the batch's read-out."""
+    """Bicubic price at (ln spot, v0) through the 4 x 4 cell centres around it of one option's (ny, nx) grid, as the
+    batch's read-out (a local Lagrange cubic along each axis)."""
     ny, nx = grid.shape
     h = 6.0 / nx
     x0 = np.log(option["strike"]) - 3.0 + 0.5 * h
     fx = (np.log(option["spot"]) - x0) / h
     fy = option["v0"] / (option["sigma"] * h) - 0.5
-    i0 = int(max(0, min(nx - 2, np.floor(fx))))
-    j0 = int(max(0, min(ny - 2, np.floor(fy))))
-    tx = min(max(fx - i0, 0.0), 1.0)
-    ty = min(max(fy - j0, 0.0), 1.0)
-    g = grid.astype(np.float64)
-    return float((1 - ty) * ((1 - tx) * g[j0, i0] + tx * g[j0, i0 + 1]) + ty * ((1 - tx) * g[j0 + 1, i0] + tx * g[j0 + 1, i0 + 1]))
+    i0, wx = _cubic(fx, nx)
+    j0, wy = _cubic(fy, ny)
+    g = grid.astype(np.float64)[j0:j0 + 4, i0:i0 + 4]
+    return float(wy @ g @ wx)
 
 
 class Calibration:
