@@ -258,6 +258,9 @@ int fe_law_digest(fe_law* law, uint64_t* out);
 int fe_law_stream(const fe_law* law, void** stream);
 /* Device time of `launches` back-to-back launches of term `term`'s fused gather pass (the roofline's kernel). */
 int fe_law_time_gather(fe_law* law, int term, int launches, float* ms);
+/* The same for stage `stage` of the term (its stored stages and tridiagonal solves, in launch order) at step dt; its
+ * kernel's name goes to `kernel` (capacity cap). FE_EINVAL when the term has no such stage. */
+int fe_law_time_stage(fe_law* law, int term, int stage, int launches, double dt, float* ms, char* kernel, size_t cap);
 
 /* ---- batched instances: one law on many uneven lattices ---------------------------------------------------------------
  * The reference batches instances as the z-planes of one lattice, all of the same nx x ny (bench/finance.py:253-288,

@@ -497,4 +497,17 @@ int fe_law_time_gather(fe_law* law, int term, int launches, float* ms)
     return fe::ok();
 }
 
+int fe_law_time_stage(fe_law* law, int term, int stage, int launches, double dt, float* ms, char* kernel, size_t cap)
+{
+    if (law == nullptr || ms == nullptr || launches < 1) return fe::fail(FE_EINVAL, "fe_law_time_stage: bad argument");
+    std::string why, name;
+    if (!law->engine.time_stage(term, stage, launches, dt, *ms, name, why)) return fe::fail(FE_EINVAL, why);
+    if (kernel != nullptr && cap > 0) {
+        const size_t n = std::min(cap - 1, name.size());
+        std::memcpy(kernel, name.data(), n);
+        kernel[n] = 0;
+    }
+    return fe::ok();
+}
+
 } // extern "C"

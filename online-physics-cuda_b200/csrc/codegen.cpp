@@ -860,13 +860,23 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
         f << "};\n}\n";
         L.kernel = "fe_tri_" + tag;
         if (axis == 0) {
-            if (nx_ > 640) {
-                why = "tridiag_x keeps a line in shared memory: nx up to 640";
-                return false;
+            const int m = (nx_ + 31) / 32;
+            if (m >= 2 && m <= kTriLaneRows) {
+                // A warp a line, M rows a lane (the partition method): lines of 33 .. 32 kTriLaneRows cells.
+                L.tri_rows = m;
+                L.smem = static_cast<unsigned>(kTriWarps * 4 * (33 * m) * 4);
+                f << "extern \"C\" __global__ void __launch_bounds__(" << 32 * kTriWarps << ") " << L.kernel
+                  << "(const __grid_constant__ FePassArgs a) { fe_tridiag_x_warp<" << ns << "::P, " << m << ", " << kTriWarps << ">(a); }\n";
+            } else {
+                if (nx_ > 640) {
+                    why = "tridiag_x keeps a line in shared memory: nx up to 640";
+                    return false;
+                }
+                L.tri_rows = 0;
+                L.smem = static_cast<unsigned>(2 * nx_ * 33 * 4);
+                f << "extern \"C\" __global__ void __launch_bounds__(32) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_tridiag_x_pass<" << ns
+                  << "::P>(a); }\n";
             }
-            L.smem = static_cast<unsigned>(2 * nx_ * 33 * 4);
-            f << "extern \"C\" __global__ void __launch_bounds__(32) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_tridiag_x_pass<" << ns
-              << "::P>(a); }\n";
         } else {
             f << "extern \"C\" __global__ void __launch_bounds__(128) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_tridiag_yz_pass<"
               << ns << "::P, " << axis << ">(a); }\n";

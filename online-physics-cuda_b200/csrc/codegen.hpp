@@ -48,7 +48,13 @@ struct Launch {
     // Net: a `half` net op on the tensor cores (128 threads a CTA, persistent); at most this many CTAs an SM hold
     // tensor memory at once (the shared memory asked for keeps more from being resident).
     int per_sm = 0;
+    // TridiagX: rows a lane of the warp-a-line partition solve (0: the 32-lines-a-block Thomas pass).
+    int tri_rows = 0;
 };
+
+// The warp-a-line x solve: up to this many rows a lane (lines of up to 32 x this many cells), this many warps a block.
+constexpr int kTriLaneRows = 16;
+constexpr int kTriWarps = 4;
 
 struct ProgramPlan {
     bool empty = true;

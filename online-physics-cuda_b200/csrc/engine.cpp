@@ -379,9 +379,16 @@ bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* r
         break;
     }
     case gen::Launch::TridiagX:
-        gx = static_cast<unsigned>((ny_ + 31) / 32);
-        gy = static_cast<unsigned>(nz_);
-        block = 32;
+        if (L.tri_rows > 0) {
+            // A warp a line (y, z), kTriWarps lines a block.
+            const unsigned long long lines = static_cast<unsigned long long>(ny_) * nz_;
+            gx = static_cast<unsigned>((lines + gen::kTriWarps - 1) / gen::kTriWarps);
+            block = 32 * gen::kTriWarps;
+        } else {
+            gx = static_cast<unsigned>((ny_ + 31) / 32);
+            gy = static_cast<unsigned>(nz_);
+            block = 32;
+        }
         smem = L.smem;
         break;
     case gen::Launch::TridiagYZ: {
@@ -907,19 +914,23 @@ bool Engine::run_program(int index, const ir::Program& p, const gen::ProgramPlan
     return true;
 }
 
+bool Engine::push_params(std::string& why)
+{
+    std::vector<float> p(1024, 0.0f);
+    for (std::size_t i = 0; i < param_host_.size() && i < 1024; ++i) p[i] = static_cast<float>(param_host_[i]);
+    if (!cuda_ok(cudaMemcpyAsync(reinterpret_cast<void*>(params_), p.data(), 1024 * sizeof(float), cudaMemcpyHostToDevice, stream_), "params", why) ||
+        !cuda_ok(cudaStreamSynchronize(stream_), "params", why)) {
+        return false;
+    }
+    params_dirty_ = false;
+    return true;
+}
+
 bool Engine::step(double dt, bool respect_max_dt, std::string& why)
 {
     if (!deferred_) violations_.clear();
     launches_ = 0;
-    if (params_dirty_) {
-        std::vector<float> p(1024, 0.0f);
-        for (std::size_t i = 0; i < param_host_.size() && i < 1024; ++i) p[i] = static_cast<float>(param_host_[i]);
-        if (!cuda_ok(cudaMemcpyAsync(reinterpret_cast<void*>(params_), p.data(), 1024 * sizeof(float), cudaMemcpyHostToDevice, stream_), "params", why) ||
-            !cuda_ok(cudaStreamSynchronize(stream_), "params", why)) {
-            return false;
-        }
-        params_dirty_ = false;
-    }
+    if (params_dirty_ && !push_params(why)) return false;
     const bool check = (steps_ % check_every_) == 0;
     PendingStep pending;
     pending.step = steps_;
@@ -1174,6 +1185,30 @@ bool Engine::time_gather(int term, int launches, float& ms, std::string& why)
     cudaEventRecord(ev0_, stream_);
     for (int i = 0; i < launches; ++i) {
         if (!launch(pp.gather, static_cast<float>(0.0), FE_PASS_AFTER | FE_PASS_RANGE, recs, why)) return false;
+    }
+    cudaEventRecord(ev1_, stream_);
+    if (!cuda_ok(cudaEventSynchronize(ev1_), "time", why)) return false;
+    return cuda_ok(cudaEventElapsedTime(&ms, ev0_, ev1_), "time", why);
+}
+
+bool Engine::time_stage(int term, int stage, int launches, double dt, float& ms, std::string& kernel, std::string& why)
+{
+    if (term < 0 || static_cast<std::size_t>(term) >= plan_.terms.size() || plan_.terms[static_cast<std::size_t>(term)].empty) {
+        why = "no such term";
+        return false;
+    }
+    const gen::ProgramPlan& pp = plan_.terms[static_cast<std::size_t>(term)];
+    if (stage < 0 || static_cast<std::size_t>(stage) >= pp.stages.size()) {
+        why = "no such stage";
+        return false;
+    }
+    const gen::Launch& L = pp.stages[static_cast<std::size_t>(stage)];
+    kernel = L.kernel;
+    if (params_dirty_ && !push_params(why)) return false;
+    FeCheck* recs[FE_MAX_OUT] = {};
+    cudaEventRecord(ev0_, stream_);
+    for (int i = 0; i < launches; ++i) {
+        if (!launch(L, static_cast<float>(dt), 0, recs, why)) return false;
     }
     cudaEventRecord(ev1_, stream_);
     if (!cuda_ok(cudaEventSynchronize(ev1_), "time", why)) return false;

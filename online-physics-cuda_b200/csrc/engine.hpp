@@ -123,6 +123,8 @@ public:
     // Times one term's gather pass alone (the measured kernel of the roofline): `launches` back-to-back launches of the
     // gather on the current state (ping-pong targets are written to their next buffer; nothing is swapped).
     bool time_gather(int term, int launches, float& ms, std::string& why);
+    // Times stage `stage` of term `term` (its stored stages and tridiagonal solves, in order) the same way, at step dt.
+    bool time_stage(int term, int stage, int launches, double dt, float& ms, std::string& kernel, std::string& why);
 
 private:
     struct RecordRef {
@@ -139,6 +141,7 @@ private:
         std::vector<std::vector<std::vector<int>>> conserves; // per term: groups of fields
     };
 
+    bool push_params(std::string& why);
     bool launch(const gen::Launch& L, float dt, int flags, FeCheck* const* recs, std::string& why, const FeCheck* const* carry = nullptr);
     bool conserved_by(int term, int field) const;
     bool launch_solve(const gen::Launch& L, float dt, std::string& why);

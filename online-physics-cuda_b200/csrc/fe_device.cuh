@@ -875,6 +875,160 @@ __device__ __forceinline__ void fe_reduce_pass(const FePassArgs& a, float* out)
     }
 }
 
+// ---- tridiagonal solves: the partition method (per-lane Thomas sweeps, PCR across lanes) -----------------------------
+
+// 1 / x by the hardware approximation (rcp.approx, about 1 ulp), for solves checked to a tolerance.
+__device__ __forceinline__ float fe_rcp(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// The reduced system of a segment of K lanes (a power of two, 2..32): lane k holds two equations, row 2k
+// (a0 x[2k-1] + b0 x[2k] + c0 x[2k+1] = d0) and row 2k+1 (a1 x[2k] + b1 x[2k+1] + c1 x[2k+2] = d1), solved by parallel
+// cyclic reduction over log2(2K) rounds of shuffles. Returns x[2k] in `first` and x[2k+1] in `last`. Every lane of the
+// warp must call it.
+__device__ __forceinline__ void fe_pcr_pairs(float a0, float b0, float c0, float d0, float a1, float b1, float c1, float d1,
+    int k, int K, float& first, float& last)
+{
+    const unsigned mask = 0xffffffffu;
+    for (int s = 1; s < 2 * K; s *= 2) {
+        const int q = s == 1 ? 1 : s / 2;
+        const bool has_lo = k - q >= 0, has_hi = k + q < K;
+        const float p0a = __shfl_up_sync(mask, s == 1 ? a1 : a0, q, K), p0b = __shfl_up_sync(mask, s == 1 ? b1 : b0, q, K);
+        const float p0c = __shfl_up_sync(mask, s == 1 ? c1 : c0, q, K), p0d = __shfl_up_sync(mask, s == 1 ? d1 : d0, q, K);
+        const float q1a = __shfl_down_sync(mask, s == 1 ? a0 : a1, q, K), q1b = __shfl_down_sync(mask, s == 1 ? b0 : b1, q, K);
+        const float q1c = __shfl_down_sync(mask, s == 1 ? c0 : c1, q, K), q1d = __shfl_down_sync(mask, s == 1 ? d0 : d1, q, K);
+        float q0a, q0b, q0c, q0d, p1a, p1b, p1c, p1d;
+        if (s == 1) {
+            q0a = a1; q0b = b1; q0c = c1; q0d = d1;
+            p1a = a0; p1b = b0; p1c = c0; p1d = d0;
+        } else {
+            q0a = __shfl_down_sync(mask, a0, q, K); q0b = __shfl_down_sync(mask, b0, q, K);
+            q0c = __shfl_down_sync(mask, c0, q, K); q0d = __shfl_down_sync(mask, d0, q, K);
+            p1a = __shfl_up_sync(mask, a1, q, K); p1b = __shfl_up_sync(mask, b1, q, K);
+            p1c = __shfl_up_sync(mask, c1, q, K); p1d = __shfl_up_sync(mask, d1, q, K);
+        }
+        // Missing neighbours are identity rows.
+        const bool lo0 = has_lo, hi0 = s == 1 ? true : has_hi, lo1 = s == 1 ? true : has_lo, hi1 = has_hi;
+        const float la0 = lo0 ? p0a : 0.f, lb0 = lo0 ? p0b : 1.f, lc0 = lo0 ? p0c : 0.f, ld0 = lo0 ? p0d : 0.f;
+        const float ua0 = hi0 ? q0a : 0.f, ub0 = hi0 ? q0b : 1.f, uc0 = hi0 ? q0c : 0.f, ud0 = hi0 ? q0d : 0.f;
+        const float la1 = lo1 ? p1a : 0.f, lb1 = lo1 ? p1b : 1.f, lc1 = lo1 ? p1c : 0.f, ld1 = lo1 ? p1d : 0.f;
+        const float ua1 = hi1 ? q1a : 0.f, ub1 = hi1 ? q1b : 1.f, uc1 = hi1 ? q1c : 0.f, ud1 = hi1 ? q1d : 0.f;
+        const float k10 = a0 * fe_rcp(lb0), k20 = c0 * fe_rcp(ub0), k11 = a1 * fe_rcp(lb1), k21 = c1 * fe_rcp(ub1);
+        const float na0 = -k10 * la0, nc0 = -k20 * uc0, nb0 = b0 - k10 * lc0 - k20 * ua0, nd0 = d0 - k10 * ld0 - k20 * ud0;
+        const float na1 = -k11 * la1, nc1 = -k21 * uc1, nb1 = b1 - k11 * lc1 - k21 * ua1, nd1 = d1 - k11 * ld1 - k21 * ud1;
+        a0 = na0; b0 = nb0; c0 = nc0; d0 = nd0;
+        a1 = na1; b1 = nb1; c1 = nc1; d1 = nd1;
+    }
+    first = d0 * fe_rcp(b0);
+    last = d1 * fe_rcp(b1);
+}
+
+// One line of n <= 32 M rows (a power-of-two K = 32 lanes, M rows a lane: lane k rows k M .. k M + M - 1) with its own
+// coefficients in every row: a[i] x[i-1] + b[i] x[i] + c[i] x[i+1] = d[i], the edge repeat already folded (a = 0 in
+// the line's first row, c = 0 in its last) and rows past the line's end the identity (a = c = d = 0, b = 1).
+// 1. Each lane eliminates inside its rows: a sweep down leaves its last row in terms of its first and the next lane's
+//    first unknown; a sweep up leaves every row in terms of the previous row, itself and the lane's last unknown.
+// 2. The lanes' first and last unknowns (a tridiagonal system of 64) by parallel cyclic reduction over shuffles.
+// 3. Each lane's interior rows by back-substitution. On return d holds the solution. Every lane of the warp calls it.
+// With M = 1 a lane would hold one row: M >= 2.
+template <int M>
+__device__ __forceinline__ void fe_tri_line(float (&a)[M], float (&b)[M], float (&c)[M], float (&d)[M], int k)
+{
+    static_assert(M >= 2, "two rows a lane at least");
+    float al = a[1], be = b[1], de = d[1];
+#pragma unroll
+    for (int r = 2; r < M; ++r) {
+        const float f = a[r] * fe_rcp(be);
+        al = -f * al;
+        be = b[r] - f * c[r - 1];
+        de = d[r] - f * de;
+    }
+    // Up, in place: b[r] becomes 1 / (row r's diagonal), c[r] the coefficient of the lane's last unknown.
+    float diag0 = b[M - 2];
+    b[M - 2] = fe_rcp(diag0);
+#pragma unroll
+    for (int r = M - 3; r >= 0; --r) {
+        const float g = c[r] * b[r + 1];
+        diag0 = b[r] - g * a[r + 1];
+        c[r] = -g * c[r + 1];
+        d[r] = d[r] - g * d[r + 1];
+        b[r] = fe_rcp(diag0);
+    }
+    float first, last;
+    fe_pcr_pairs(a[0], diag0, c[0], d[0], al, be, c[M - 1], de, k, 32, first, last);
+    float prev = first;
+    d[0] = first;
+#pragma unroll
+    for (int r = 1; r < M - 1; ++r) {
+        prev = (d[r] - a[r] * prev - c[r] * last) * b[r];
+        d[r] = prev;
+    }
+    d[M - 1] = last;
+}
+
+// Tridiagonal solves along x, a warp a line (the partition method, fe_tri_line; M = ceil(NX / 32) rows a lane): the
+// warp forms the line's coefficients 32 consecutive cells at a time (coalesced reads), stages them in its shared
+// memory (padded one word in 32 so a lane's M consecutive rows fall in different banks), each lane takes its M rows,
+// the warp solves, and the answer goes back out through the same staging, coalesced. Lines: NY * NZ, WARPS a block.
+template <class P, int M, int WARPS>
+__device__ __forceinline__ void fe_tridiag_x_warp(const FePassArgs& a)
+{
+    constexpr int S = 32 * M + M; // a staged row of 32 M cells, padded
+    extern __shared__ __align__(128) float fe_sm[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    float* sa = fe_sm + warp * 4 * S;
+    float* sb = sa + S;
+    float* sc = sb + S;
+    float* sd = sc + S;
+    const fe_u64 line = static_cast<fe_u64>(blockIdx.x) * WARPS + warp;
+    if (line >= static_cast<fe_u64>(P::NY) * P::NZ) return; // a whole warp leaves together
+    const int y = static_cast<int>(line % P::NY);
+    const int z = static_cast<int>(line / P::NY);
+    FePlainCtx<P> ctx;
+    ctx.src = a.src;
+    ctx.dt = a.dt;
+    auto pad = [](int i) { return i + (i >> 5); };
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        const int x = i * 32 + lane;
+        float lo = 0.f, di = 1.f, up = 0.f, rhs = 0.f;
+        if (x < P::NX) {
+            P::coef(ctx, x, y, z, lo, di, up, rhs);
+            if (x == 0) { di += lo; lo = 0.f; }
+            if (x + 1 == P::NX) { di += up; up = 0.f; }
+        }
+        sa[pad(x)] = lo;
+        sb[pad(x)] = di;
+        sc[pad(x)] = up;
+        sd[pad(x)] = rhs;
+    }
+    __syncwarp();
+    float ra[M], rb[M], rc[M], rd[M];
+#pragma unroll
+    for (int r = 0; r < M; ++r) {
+        const int i = pad(lane * M + r);
+        ra[r] = sa[i];
+        rb[r] = sb[i];
+        rc[r] = sc[i];
+        rd[r] = sd[i];
+    }
+    fe_tri_line<M>(ra, rb, rc, rd, lane);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < M; ++r) sd[pad(lane * M + r)] = rd[r];
+    __syncwarp();
+    float* out = a.out[0] + (static_cast<fe_u64>(z) * P::NY + y) * P::NX;
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        const int x = i * 32 + lane;
+        if (x < P::NX) out[x] = sd[pad(x)];
+    }
+}
+
 // Tridiagonal solves along x, 32 lines a block (32 consecutive y at one z): coefficient tiles come in coalesced through
 // shared memory, each thread runs Thomas' recurrence on its line (in the reference's order: the edge cell repeating, its
 // missing neighbour's coefficient landing on the diagonal), keeping c' and d' for the whole line in shared memory, so

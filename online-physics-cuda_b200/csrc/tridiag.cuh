@@ -16,13 +16,8 @@
 
 #if defined(__CUDACC__) || defined(__CUDACC_RTC__)
 
-// 1 / x by the hardware approximation (rcp.approx, about 1 ulp), for solves checked to a tolerance.
-__device__ __forceinline__ float fe_rcp(float x)
-{
-    float r;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
+// fe_rcp and fe_pcr_pairs (the reduced system's parallel cyclic reduction) live in fe_device.cuh, which the law's
+// generated passes share; this file adds the constant-coefficient row solves of the batched Heston kernel.
 
 // Thomas over the first n <= M rows held by one thread, the same (a, b, c) in every row and the edge repeat folded at
 // the line's two ends (b + a in row 0 with no a; b + c in row n-1 with no c).
@@ -54,47 +49,6 @@ __device__ __forceinline__ void fe_thomas_row(float a, float b, float c, float (
             d[i] = next;
         }
     }
-}
-
-// The reduced system of a segment of K lanes (a power of two, 2..32): lane k holds two equations, row 2k
-// (a0 x[2k-1] + b0 x[2k] + c0 x[2k+1] = d0) and row 2k+1 (a1 x[2k] + b1 x[2k+1] + c1 x[2k+2] = d1), solved by parallel
-// cyclic reduction over log2(2K) rounds of shuffles. Returns x[2k] in `first` and x[2k+1] in `last`. Every lane of the
-// warp must call it.
-__device__ __forceinline__ void fe_pcr_pairs(float a0, float b0, float c0, float d0, float a1, float b1, float c1, float d1,
-    int k, int K, float& first, float& last)
-{
-    const unsigned mask = 0xffffffffu;
-    for (int s = 1; s < 2 * K; s *= 2) {
-        const int q = s == 1 ? 1 : s / 2;
-        const bool has_lo = k - q >= 0, has_hi = k + q < K;
-        const float p0a = __shfl_up_sync(mask, s == 1 ? a1 : a0, q, K), p0b = __shfl_up_sync(mask, s == 1 ? b1 : b0, q, K);
-        const float p0c = __shfl_up_sync(mask, s == 1 ? c1 : c0, q, K), p0d = __shfl_up_sync(mask, s == 1 ? d1 : d0, q, K);
-        const float q1a = __shfl_down_sync(mask, s == 1 ? a0 : a1, q, K), q1b = __shfl_down_sync(mask, s == 1 ? b0 : b1, q, K);
-        const float q1c = __shfl_down_sync(mask, s == 1 ? c0 : c1, q, K), q1d = __shfl_down_sync(mask, s == 1 ? d0 : d1, q, K);
-        float q0a, q0b, q0c, q0d, p1a, p1b, p1c, p1d;
-        if (s == 1) {
-            q0a = a1; q0b = b1; q0c = c1; q0d = d1;
-            p1a = a0; p1b = b0; p1c = c0; p1d = d0;
-        } else {
-            q0a = __shfl_down_sync(mask, a0, q, K); q0b = __shfl_down_sync(mask, b0, q, K);
-            q0c = __shfl_down_sync(mask, c0, q, K); q0d = __shfl_down_sync(mask, d0, q, K);
-            p1a = __shfl_up_sync(mask, a1, q, K); p1b = __shfl_up_sync(mask, b1, q, K);
-            p1c = __shfl_up_sync(mask, c1, q, K); p1d = __shfl_up_sync(mask, d1, q, K);
-        }
-        // Missing neighbours are identity rows.
-        const bool lo0 = has_lo, hi0 = s == 1 ? true : has_hi, lo1 = s == 1 ? true : has_lo, hi1 = has_hi;
-        const float la0 = lo0 ? p0a : 0.f, lb0 = lo0 ? p0b : 1.f, lc0 = lo0 ? p0c : 0.f, ld0 = lo0 ? p0d : 0.f;
-        const float ua0 = hi0 ? q0a : 0.f, ub0 = hi0 ? q0b : 1.f, uc0 = hi0 ? q0c : 0.f, ud0 = hi0 ? q0d : 0.f;
-        const float la1 = lo1 ? p1a : 0.f, lb1 = lo1 ? p1b : 1.f, lc1 = lo1 ? p1c : 0.f, ld1 = lo1 ? p1d : 0.f;
-        const float ua1 = hi1 ? q1a : 0.f, ub1 = hi1 ? q1b : 1.f, uc1 = hi1 ? q1c : 0.f, ud1 = hi1 ? q1d : 0.f;
-        const float k10 = a0 * fe_rcp(lb0), k20 = c0 * fe_rcp(ub0), k11 = a1 * fe_rcp(lb1), k21 = c1 * fe_rcp(ub1);
-        const float na0 = -k10 * la0, nc0 = -k20 * uc0, nb0 = b0 - k10 * lc0 - k20 * ua0, nd0 = d0 - k10 * ld0 - k20 * ud0;
-        const float na1 = -k11 * la1, nc1 = -k21 * uc1, nb1 = b1 - k11 * lc1 - k21 * ua1, nd1 = d1 - k11 * ld1 - k21 * ud1;
-        a0 = na0; b0 = nb0; c0 = nc0; d0 = nd0;
-        a1 = na1; b1 = nb1; c1 = nc1; d1 = nd1;
-    }
-    first = d0 * fe_rcp(b0);
-    last = d1 * fe_rcp(b1);
 }
 
 // A line with the same (a, b, c) in every row, the edge repeat folded at its two ends: the x lines of a row of a law

@@ -164,6 +164,7 @@ SIGNATURES = {
     "fe_law_digest": (_i, [_p, _c.POINTER(_c.c_uint64)]),
     "fe_law_stream": (_i, [_p, _c.POINTER(_p)]),
     "fe_law_time_gather": (_i, [_p, _i, _i, _c.POINTER(_c.c_float)]),
+    "fe_law_time_stage": (_i, [_p, _i, _i, _i, _d, _c.POINTER(_c.c_float), _p, _s]),
     "fe_batch_create": (_i, [_cs, _c.POINTER(fe_batch_desc), _i, _c.POINTER(_p)]),
     "fe_batch_destroy": (None, [_p]),
     "fe_batch_plan": (_i, [_cs, _c.POINTER(fe_batch_desc), _i, _c.POINTER(_i), _c.POINTER(_i), _p, _p]),

@@ -235,6 +235,13 @@ class Solver:
         return [{"step": e.step, "term": e.term, "group": e.group, "substeps": e.substeps, "before": e.before, "after": e.after,
                  "scale": e.scale} for e in buf[:n.value]]
 
+    def time_stage(self, term=0, stage=0, launches=10, dt=0.0):
+        """(kernel name, ms for `launches` back-to-back launches of the term's stage `stage`)."""
+        ms = ctypes.c_float()
+        name = ctypes.create_string_buffer(128)
+        _lib.check(self._lib.fe_law_time_stage(self._h, term, stage, launches, float(dt), ctypes.byref(ms), name, 128))
+        return name.value.decode(), ms.value
+
     def time_gather(self, term=0, launches=10):
         ms = ctypes.c_float()
         _lib.check(self._lib.fe_law_time_gather(self._h, term, launches, ctypes.byref(ms)))
