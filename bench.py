@@ -775,6 +775,35 @@ def nets_section(stream_sync):
 HESTON_CALIB = os.path.join(ROOT, "tests", "golden", "heston", "calib_512.npz")
 
 
+def tridiag_section():
+    """The law's tridiagonal solves timed alone (fe_law_time_stage): tests/laws/heston_douglas.law on the calibration's
+    lattice (256 x 128 x 512 planes, one option a plane): its stages in launch order (the stored explicit rate, the
+    x solve by the partition method, the y solve a thread a line), each launched 10 times back to back. Cells solved a
+    second, and the effective bandwidth at 8 B a cell (the right-hand side read, the answer written; the coefficients
+    are formed from static fields in the same kernel and read on top of that)."""
+    import numpy as np
+    from fieldcuda.heston import lattice_fields, sample_options
+    from fieldcuda.solver import Solver
+    nx, ny, nz = 256, 128, 512
+    fields, h = lattice_fields(sample_options(nz, 9, sizes=((nx, ny),)), nx, ny)
+    s = Solver(open(HESTON_DOUGLAS_LAW).read(), nx, ny, nz, h, "heston_douglas.law")
+    for k, v in fields.items():
+        s.set_field(k, v)
+    s.step(1.0 / 512)
+    out = {"lattice": f"{nx} x {ny} x {nz}", "stages": []}
+    cells = nx * ny * nz
+    for stage in range(16):
+        try:
+            name, ms = s.time_stage(0, stage, 10, 1.0 / 512)
+        except Exception:
+            break
+        per = ms / 10
+        out["stages"].append({"kernel": name, "ms": per, "cells_per_s": cells / (per * 1e-3),
+                              "gbs_at_8_bytes_a_cell": 8 * cells / (per * 1e-3) / 1e9})
+    s.close()
+    return out
+
+
 def calibration_section():
     """The adjoint calibration: loss = sum (price - target)^2 over 512 options (one maturity, strikes U[80, 120]) on one
     256 x 128 lattice (the options as its z-planes), 512 Douglas ADI steps, and its gradient with respect to (kappa,
@@ -1077,9 +1106,10 @@ def run_ours(args, world, rank, local):
     multifield = None
     if not args.no_multifield:
         multifield = multifield_section(256, 10, 3, torch.cuda.synchronize)
-    calibration = None
+    calibration = tridiag = None
     if not args.no_calibration:
         calibration = calibration_section()
+        tridiag = tridiag_section()
     learned = None
     if not args.no_learned:
         learned = fhn_learned_section()
@@ -1122,6 +1152,7 @@ def run_ours(args, world, rank, local):
         "heston_batch": heston,
         "multifield_256": multifield,
         "adjoint_calibration": calibration,
+        "tridiag_solves": tridiag,
         "fhn_learned": learned,
         "nets_half": nets,
     }))
