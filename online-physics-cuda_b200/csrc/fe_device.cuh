@@ -889,9 +889,11 @@ __device__ __forceinline__ float fe_rcp(float x)
 // (a0 x[2k-1] + b0 x[2k] + c0 x[2k+1] = d0) and row 2k+1 (a1 x[2k] + b1 x[2k+1] + c1 x[2k+2] = d1), solved by parallel
 // cyclic reduction over log2(2K) rounds of shuffles. Returns x[2k] in `first` and x[2k+1] in `last`. Every lane of the
 // warp must call it.
+template <bool RN = false>
 __device__ __forceinline__ void fe_pcr_pairs(float a0, float b0, float c0, float d0, float a1, float b1, float c1, float d1,
     int k, int K, float& first, float& last)
 {
+    auto rcp = [](float x) { return RN ? __frcp_rn(x) : fe_rcp(x); };
     const unsigned mask = 0xffffffffu;
     for (int s = 1; s < 2 * K; s *= 2) {
         const int q = s == 1 ? 1 : s / 2;
@@ -916,14 +918,14 @@ __device__ __forceinline__ void fe_pcr_pairs(float a0, float b0, float c0, float
         const float ua0 = hi0 ? q0a : 0.f, ub0 = hi0 ? q0b : 1.f, uc0 = hi0 ? q0c : 0.f, ud0 = hi0 ? q0d : 0.f;
         const float la1 = lo1 ? p1a : 0.f, lb1 = lo1 ? p1b : 1.f, lc1 = lo1 ? p1c : 0.f, ld1 = lo1 ? p1d : 0.f;
         const float ua1 = hi1 ? q1a : 0.f, ub1 = hi1 ? q1b : 1.f, uc1 = hi1 ? q1c : 0.f, ud1 = hi1 ? q1d : 0.f;
-        const float k10 = a0 * fe_rcp(lb0), k20 = c0 * fe_rcp(ub0), k11 = a1 * fe_rcp(lb1), k21 = c1 * fe_rcp(ub1);
+        const float k10 = a0 * rcp(lb0), k20 = c0 * rcp(ub0), k11 = a1 * rcp(lb1), k21 = c1 * rcp(ub1);
         const float na0 = -k10 * la0, nc0 = -k20 * uc0, nb0 = b0 - k10 * lc0 - k20 * ua0, nd0 = d0 - k10 * ld0 - k20 * ud0;
         const float na1 = -k11 * la1, nc1 = -k21 * uc1, nb1 = b1 - k11 * lc1 - k21 * ua1, nd1 = d1 - k11 * ld1 - k21 * ud1;
         a0 = na0; b0 = nb0; c0 = nc0; d0 = nd0;
         a1 = na1; b1 = nb1; c1 = nc1; d1 = nd1;
     }
-    first = d0 * fe_rcp(b0);
-    last = d1 * fe_rcp(b1);
+    first = d0 * rcp(b0);
+    last = d1 * rcp(b1);
 }
 
 // One line of n <= 32 M rows (a power-of-two K = 32 lanes, M rows a lane: lane k rows k M .. k M + M - 1) with its own
@@ -933,6 +935,7 @@ __device__ __forceinline__ void fe_pcr_pairs(float a0, float b0, float c0, float
 //    first unknown; a sweep up leaves every row in terms of the previous row, itself and the lane's last unknown.
 // 2. The lanes' first and last unknowns (a tridiagonal system of 64) by parallel cyclic reduction over shuffles.
 // 3. Each lane's interior rows by back-substitution. On return d holds the solution. Every lane of the warp calls it.
+// Reciprocals are correctly rounded (the law's own solves are held to the reference's CPU solver to a tolerance).
 // With M = 1 a lane would hold one row: M >= 2.
 template <int M>
 __device__ __forceinline__ void fe_tri_line(float (&a)[M], float (&b)[M], float (&c)[M], float (&d)[M], int k)
@@ -941,24 +944,24 @@ __device__ __forceinline__ void fe_tri_line(float (&a)[M], float (&b)[M], float 
     float al = a[1], be = b[1], de = d[1];
 #pragma unroll
     for (int r = 2; r < M; ++r) {
-        const float f = a[r] * fe_rcp(be);
+        const float f = a[r] * __frcp_rn(be);
         al = -f * al;
         be = b[r] - f * c[r - 1];
         de = d[r] - f * de;
     }
     // Up, in place: b[r] becomes 1 / (row r's diagonal), c[r] the coefficient of the lane's last unknown.
     float diag0 = b[M - 2];
-    b[M - 2] = fe_rcp(diag0);
+    b[M - 2] = __frcp_rn(diag0);
 #pragma unroll
     for (int r = M - 3; r >= 0; --r) {
         const float g = c[r] * b[r + 1];
         diag0 = b[r] - g * a[r + 1];
         c[r] = -g * c[r + 1];
         d[r] = d[r] - g * d[r + 1];
-        b[r] = fe_rcp(diag0);
+        b[r] = __frcp_rn(diag0);
     }
     float first, last;
-    fe_pcr_pairs(a[0], diag0, c[0], d[0], al, be, c[M - 1], de, k, 32, first, last);
+    fe_pcr_pairs<true>(a[0], diag0, c[0], d[0], al, be, c[M - 1], de, k, 32, first, last);
     float prev = first;
     d[0] = first;
 #pragma unroll

@@ -163,11 +163,27 @@ def price_at(grid, option):
     return float(wy @ g @ wx)
 
 
+def price_bilinear(grid, option):
+    """Bilinear price at (ln spot, v0) between the four cell centres around it (clamped to the grid): the calibration's
+    read-out (Calibration.prices), kept bilinear so its gradient through autograd is the read-out's own."""
+    ny, nx = grid.shape
+    h = 6.0 / nx
+    x0 = np.log(option["strike"]) - 3.0 + 0.5 * h
+    fx = (np.log(option["spot"]) - x0) / h
+    fy = option["v0"] / (option["sigma"] * h) - 0.5
+    i0 = int(max(0, min(nx - 2, np.floor(fx))))
+    j0 = int(max(0, min(ny - 2, np.floor(fy))))
+    tx = min(max(fx - i0, 0.0), 1.0)
+    ty = min(max(fy - j0, 0.0), 1.0)
+    g = grid.astype(np.float64)
+    return float((1 - ty) * ((1 - tx) * g[j0, i0] + tx * g[j0, i0 + 1]) + ty * ((1 - tx) * g[j0 + 1, i0] + tx * g[j0 + 1, i0 + 1]))
+
+
 class Calibration:
     """The Heston calibration's loss and its gradient by reverse mode through the ADI law (the reference's adjoint
     calibration, bench/calibrate.py, there through the explicit law): the options of one maturity as the z-planes of
     one (nx, ny) lattice, stepped by tests/laws/heston_douglas.law's scheme (`law_text`), the price read off each plane
-    by the batch's bilinear interpolation, loss = sum (price - target)^2, gradient with respect to (kappa, theta,
+    by bilinear interpolation (price_bilinear), loss = sum (price - target)^2, gradient with respect to (kappa, theta,
     sigma, rho, v0) through LawSteps (the IR-generated adjoint law, sqrt(N) checkpoints) and torch autograd for the
     rest (the variance rows sigma (j + 1/2) h and the read-out at v0)."""
 

@@ -135,8 +135,8 @@ def test_calibration_gradient_matches_fp64_central_differences(cuda):
             VT = o.fields["V"]
         finally:
             law_cpu.F32 = old
-        from fieldcuda.heston import price_at
-        p = np.array([price_at(VT[i].astype(np.float64), o_) for i, o_ in enumerate(opts)], np.float64)
+        from fieldcuda.heston import price_bilinear
+        p = np.array([price_bilinear(VT[i].astype(np.float64), o_) for i, o_ in enumerate(opts)], np.float64)
         return float(np.sum((p - z["targets"]) ** 2))
 
     for i in range(5):
