@@ -1168,6 +1168,9 @@ def profile_case(name):
     multifield  the 43-term law on 128^3, 3 steps: its generated passes;
     calibration the adjoint calibration's lattice (512 options, 256 x 128) over 4 Douglas steps: one loss and gradient
                 (the forward, the checkpointed recompute and the adjoint law's steps);
+    tridiag     tests/laws/heston_douglas.law on 256 x 128 x 256 (256 options; 32 MiB a buffer, the law's buffers
+                together larger than L2), 3 steps: the x solve by the partition method
+                (fe_tri_* with fe_tridiag_x_warp) and the y solve;
     nets        the learned-flux and learned-conduction laws (tests/laws/nets_flux.law, nets_ldiffuse.law) on
                 128 x 128 x 64, 3 steps each with fp32 nets, then with the nets declared half: the tcgen05 net stages."""
     import numpy as np
@@ -1228,6 +1231,19 @@ def profile_case(name):
         torch.cuda.synchronize()
         cal.close()
         print(json.dumps({"case": name, "loss": loss, "grad": [float(g) for g in grad]}))
+    elif name == "tridiag":
+        from fieldcuda.heston import lattice_fields, sample_options
+        from fieldcuda.solver import Solver
+        nx, ny, nz = 256, 128, 256
+        fields, h = lattice_fields(sample_options(nz, 9, sizes=((nx, ny),)), nx, ny)
+        s = Solver(open(HESTON_DOUGLAS_LAW).read(), nx, ny, nz, h, "heston_douglas.law")
+        for k, v in fields.items():
+            s.set_field(k, v)
+        for _ in range(3):
+            s.step(1.0 / 512)
+        s.sync()
+        print(json.dumps({"case": name, "violations": len(s.violations())}))
+        s.close()
     elif name == "nets":
         from fieldcuda.solver import Solver
         os.chdir(ROOT)  # the laws' weight files are repository paths
@@ -1266,7 +1282,7 @@ def main():
     ap.add_argument("--no-nets", action="store_true", help="skip the net ops section (fp32 and tensor-core nets)")
     ap.add_argument("--no-calibration", action="store_true", help="skip the adjoint calibration section")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-correction section")
-    ap.add_argument("--profile-case", default="", help="run one small case for ncu (heat, heston, corrector, multifield, nets) and exit")
+    ap.add_argument("--profile-case", default="", help="run one small case for ncu (heat, heat256, heston, corrector, multifield, calibration, tridiag, nets) and exit")
     args = ap.parse_args()
     if args.profile_case:
         profile_case(args.profile_case)

@@ -647,6 +647,19 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
         // plane (RZ = 0) starts at 2 stages: the explicit Heston gather (7 sources, 512 x 256) takes 0.39 ms a substep
         // on 128 planes with 2 stages against 0.65 with 4, which leave room for one CTA an SM only.
         const int shallowest = rz == 0 ? 2 : std::max(4, 2 * rz + 2);
+        // First, 32-row tiles when they leave room for 3 CTAs an SM (a warp then computes 4 rows of a plane, so the
+        // per-plane waits, barrier and ring bookkeeping are shared by 16 cells a lane): the 512^3 heat gather, 16-row
+        // tiles 4.15 TB/s (5 CTAs an SM), 24 rows 4.10, 32 rows 4.41 (3 CTAs), 32 rows with 5 stages 4.02, 40 rows 3.34.
+        {
+            std::size_t floats = 0;
+            for (const Source& s : pb.sources) floats += static_cast<std::size_t>(((128 + 2 * s.ax) * (32 + 2 * s.ry) + 31) / 32 * 32) * shallowest;
+            if (floats * 4 <= 75u * 1024 && 32 + 2 * rz < 256) {
+                L.ty = 32;
+                L.nst = shallowest;
+                L.smem = static_cast<unsigned>(floats * 4);
+                return true;
+            }
+        }
         for (const std::size_t budget : {72u * 1024, 110u * 1024, 200u * 1024}) {
             for (const int ty : {16, 8}) {
                 for (int nst = shallowest; nst <= shallowest + 2; ++nst) {

@@ -418,7 +418,9 @@ bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* r
         std::any_of(L.checked_fields.begin(), L.checked_fields.end(), [](int f) { return f >= 0; })) {
         name += "_halo";
     }
-    if (L.kind != gen::Launch::Net && static_cast<std::size_t>(a.blocks) * 4 * FE_MAX_OUT > partial_doubles_) {
+    // Passes and reductions keep per-block partial sums; the solves and net stages keep none.
+    const bool partials = L.kind == gen::Launch::Pass || L.kind == gen::Launch::Reduce;
+    if (partials && static_cast<std::size_t>(a.blocks) * 4 * FE_MAX_OUT > partial_doubles_) {
         why = "internal: too few partial sums for a launch";
         return false;
     }

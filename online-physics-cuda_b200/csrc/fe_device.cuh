@@ -154,6 +154,27 @@ __device__ __forceinline__ double fe_warp_sum(double v)
     return v;
 }
 
+// Neumaier's compensated summation: c collects what adding x to s rounds away (the larger magnitude's error term), so
+// s + c is the sum to about one rounding whatever the order of magnitudes. Used in a fixed order everywhere, so two
+// runs still agree to the bit.
+__device__ __forceinline__ void fe_kahan_add(double& s, double& c, double x)
+{
+    const double t = s + x;
+    c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+}
+
+// A compensated sum (s, c) over a warp in the fixed tree (16, 8, 4, 2, 1), folded to one double.
+__device__ __forceinline__ double fe_warp_sum_c(double s, double c)
+{
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ps = __shfl_down_sync(0xffffffffu, s, o);
+        c += __shfl_down_sync(0xffffffffu, c, o);
+        fe_kahan_add(s, c, ps);
+    }
+    return s + c;
+}
+
 __device__ __forceinline__ unsigned fe_warp_min(unsigned v)
 {
     for (int o = 16; o > 0; o >>= 1) {
@@ -174,10 +195,12 @@ __device__ __forceinline__ unsigned fe_warp_max(unsigned v)
 
 // Per-thread contract accumulators of one checked field in a gather pass. Totals are FP64; each group of 4 cells a lane
 // owns is first summed in fp32 ((c0 + c1) + (c2 + c3)), whose rounding (a few 1e-8 of the group) is far below the
-// conservation tolerance (1e-5 of the total of |field|). Bounds are float min/max (NaN ignored), turned into ordered
+// conservation tolerance (1e-5 of the total of |field|). From there on the totals compared for conservation are
+// compensated (Neumaier, fe_kahan_add) at every level: a lane's planes, the warp tree, the block's warps, the blocks. Bounds are float min/max (NaN ignored), turned into ordered
 // keys once per block.
 struct FeAcc {
     double before, before_abs, after, after_abs;
+    double before_c, after_c;  // compensation of before and after (fe_kahan_add)
     float pb, pba, pa;  // this plane's fp32 partials of before, |before| and after (fe_acc_flush moves them to FP64)
     float lo, hi;
     unsigned bad, nan, first, changed;
@@ -186,6 +209,7 @@ struct FeAcc {
 __device__ __forceinline__ void fe_acc_init(FeAcc& a)
 {
     a.before = 0.0; a.before_abs = 0.0; a.after = 0.0; a.after_abs = 0.0;
+    a.before_c = 0.0; a.after_c = 0.0;
     a.pb = 0.f; a.pba = 0.f; a.pa = 0.f;
     a.lo = __int_as_float(0x7f800000); a.hi = __int_as_float(0xff800000);
     a.bad = 0u; a.nan = 0u; a.first = 0u; a.changed = 0u;
@@ -195,9 +219,9 @@ __device__ __forceinline__ void fe_acc_init(FeAcc& a)
 // the FP64 totals. Called once a plane, in a fixed order.
 __device__ __forceinline__ void fe_acc_flush(FeAcc& a)
 {
-    a.before += static_cast<double>(a.pb);
+    fe_kahan_add(a.before, a.before_c, static_cast<double>(a.pb));
     a.before_abs += static_cast<double>(a.pba);
-    a.after += static_cast<double>(a.pa);
+    fe_kahan_add(a.after, a.after_c, static_cast<double>(a.pa));
     a.pb = 0.f; a.pba = 0.f; a.pa = 0.f;
 }
 
@@ -249,11 +273,11 @@ __device__ __forceinline__ void fe_acc_cell(FeAcc& a, float before, float after,
     bool totals_before, bool totals_after, bool range = true)
 {
     if (totals_before) {
-        a.before += static_cast<double>(before);
+        fe_kahan_add(a.before, a.before_c, static_cast<double>(before));
         a.before_abs += static_cast<double>(fabsf(before));
     }
     if (totals_after) {
-        a.after += static_cast<double>(after);
+        fe_kahan_add(a.after, a.after_c, static_cast<double>(after));
     }
     if (range) {
         a.lo = fminf(a.lo, after);
@@ -271,6 +295,7 @@ __device__ __forceinline__ void fe_acc_cell(FeAcc& a, float before, float after,
 // its bad cells are counted in the block's shared `fails` (out of range, not finite, ~index of the first).
 struct FeOutAcc {
     double after, after_abs;
+    double after_c;  // compensation of after (fe_kahan_add)
     float pa, paa;  // this plane's fp32 partials of after and |after|
     float lo, hi;   // least and most value so far (NaN ignored)
     unsigned changed;
@@ -278,7 +303,7 @@ struct FeOutAcc {
 
 __device__ __forceinline__ void fe_out_init(FeOutAcc& a)
 {
-    a.after = 0.0; a.after_abs = 0.0;
+    a.after = 0.0; a.after_abs = 0.0; a.after_c = 0.0;
     a.pa = 0.f; a.paa = 0.f;
     a.lo = __int_as_float(0x7f800000); a.hi = __int_as_float(0xff800000);
     a.changed = 0u;
@@ -306,7 +331,7 @@ __device__ __forceinline__ void fe_out_row4(FeOutAcc& a, const float* before, co
 __device__ __forceinline__ bool fe_out_plane(FeOutAcc& a, float lo, float hi, bool range)
 {
     const bool suspect = range && !(a.lo >= lo && a.hi <= hi && fabsf(a.pa) <= 3.0e38f);
-    a.after += static_cast<double>(a.pa);
+    fe_kahan_add(a.after, a.after_c, static_cast<double>(a.pa));
     a.after_abs += static_cast<double>(a.paa);
     a.pa = 0.f;
     a.paa = 0.f;
@@ -323,7 +348,7 @@ __device__ __forceinline__ void fe_out_bad(unsigned* fails, float v, unsigned in
 __device__ __forceinline__ void fe_out_cell(FeOutAcc& a, float before, float after, float lo, float hi, unsigned index, bool range,
     unsigned* fails)
 {
-    a.after += static_cast<double>(after);
+    fe_kahan_add(a.after, a.after_c, static_cast<double>(after));
     a.after_abs += static_cast<double>(fabsf(after));
     if (range) {
         a.lo = fminf(a.lo, after);
@@ -340,7 +365,7 @@ __device__ __forceinline__ void fe_out_block(FeOutAcc& a, double* scratch, doubl
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int warps = (blockDim.x + 31) >> 5;
-    const double s2 = fe_warp_sum(a.after);
+    const double s2 = fe_warp_sum_c(a.after, a.after_c);
     const double s3 = fe_warp_sum(a.after_abs);
     const unsigned lo = fe_warp_min(a.lo <= a.hi ? fe_order_key(a.lo) : 0xffffffffu);
     const unsigned hi = fe_warp_max(a.lo <= a.hi ? fe_order_key(a.hi) : 0u);
@@ -354,11 +379,12 @@ __device__ __forceinline__ void fe_out_block(FeOutAcc& a, double* scratch, doubl
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t2 = 0.0, t3 = 0.0;
+        double t2 = 0.0, t3 = 0.0, c2 = 0.0;
         for (int w = 0; w < warps; ++w) {
-            t2 += scratch[4 * w + 2];
+            fe_kahan_add(t2, c2, scratch[4 * w + 2]);
             t3 += scratch[4 * w + 3];
         }
+        t2 += c2;
         partial[0] = 0.0;
         partial[1] = 0.0;
         partial[2] = t2;
@@ -377,9 +403,9 @@ __device__ __forceinline__ void fe_acc_block(FeAcc& a, double* scratch, double* 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int warps = (blockDim.x + 31) >> 5;
-    const double s0 = fe_warp_sum(a.before);
+    const double s0 = fe_warp_sum_c(a.before, a.before_c);
     const double s1 = fe_warp_sum(a.before_abs);
-    const double s2 = fe_warp_sum(a.after);
+    const double s2 = fe_warp_sum_c(a.after, a.after_c);
     const double s3 = fe_warp_sum(a.after_abs);
     // Float bounds to ordered keys (no finite-or-infinite value seen: the empty keys).
     const unsigned lo = fe_warp_min(a.lo <= a.hi ? fe_order_key(a.lo) : 0xffffffffu);
@@ -402,13 +428,15 @@ __device__ __forceinline__ void fe_acc_block(FeAcc& a, double* scratch, double* 
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+        double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0, c0 = 0.0, c2 = 0.0;
         for (int w = 0; w < warps; ++w) {
-            t0 += scratch[4 * w + 0];
+            fe_kahan_add(t0, c0, scratch[4 * w + 0]);
             t1 += scratch[4 * w + 1];
-            t2 += scratch[4 * w + 2];
+            fe_kahan_add(t2, c2, scratch[4 * w + 2]);
             t3 += scratch[4 * w + 3];
         }
+        t0 += c0;
+        t2 += c2;
         partial[0] = t0;
         partial[1] = t1;
         partial[2] = t2;
@@ -435,21 +463,21 @@ __device__ __forceinline__ void fe_acc_finish(const double* partials, int blocks
     }
     __threadfence();
     // Thread t sums blocks t, t + T, t + 2T, ... in order; then a fixed tree over the threads.
-    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0, c0 = 0.0, c1 = 0.0, c2 = 0.0, c3 = 0.0;
     for (int b = threadIdx.x; b < blocks; b += blockDim.x) {
         const volatile double* p = partials + 4 * b;
-        t0 += p[0];
-        t1 += p[1];
-        t2 += p[2];
-        t3 += p[3];
+        fe_kahan_add(t0, c0, p[0]);
+        fe_kahan_add(t1, c1, p[1]);
+        fe_kahan_add(t2, c2, p[2]);
+        fe_kahan_add(t3, c3, p[3]);
     }
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int warps = (blockDim.x + 31) >> 5;
-    t0 = fe_warp_sum(t0);
-    t1 = fe_warp_sum(t1);
-    t2 = fe_warp_sum(t2);
-    t3 = fe_warp_sum(t3);
+    t0 = fe_warp_sum_c(t0, c0);
+    t1 = fe_warp_sum_c(t1, c1);
+    t2 = fe_warp_sum_c(t2, c2);
+    t3 = fe_warp_sum_c(t3, c3);
     __syncthreads();
     if (lane == 0) {
         scratch[4 * warp + 0] = t0;
@@ -459,13 +487,17 @@ __device__ __forceinline__ void fe_acc_finish(const double* partials, int blocks
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0, k0 = 0.0, k1 = 0.0, k2 = 0.0, k3 = 0.0;
         for (int w = 0; w < warps; ++w) {
-            s0 += scratch[4 * w + 0];
-            s1 += scratch[4 * w + 1];
-            s2 += scratch[4 * w + 2];
-            s3 += scratch[4 * w + 3];
+            fe_kahan_add(s0, k0, scratch[4 * w + 0]);
+            fe_kahan_add(s1, k1, scratch[4 * w + 1]);
+            fe_kahan_add(s2, k2, scratch[4 * w + 2]);
+            fe_kahan_add(s3, k3, scratch[4 * w + 3]);
         }
+        s0 += k0;
+        s1 += k1;
+        s2 += k2;
+        s3 += k3;
         if (carry != nullptr) {
             // The totals after the pass that last wrote the field are the totals before this one.
             rec->before = carry->after;

@@ -27,16 +27,16 @@ __global__ void __launch_bounds__(256) totals_f32(const float* __restrict__ v, s
     fe_acc_init(acc);
     if (blockIdx.x == 0 && threadIdx.x < head) {
         const double x = static_cast<double>(v[threadIdx.x]);
-        acc.before += x;
+        fe_kahan_add(acc.before, acc.before_c, x);
         acc.before_abs += fabs(x);
     }
 #pragma unroll 4
     for (size_t i = b0 / 4 + threadIdx.x; i < b1 / 4; i += blockDim.x) {
         const float4 x = __ldg(w4 + i);
-        acc.before += static_cast<double>(x.x);
-        acc.before += static_cast<double>(x.y);
-        acc.before += static_cast<double>(x.z);
-        acc.before += static_cast<double>(x.w);
+        fe_kahan_add(acc.before, acc.before_c, static_cast<double>(x.x));
+        fe_kahan_add(acc.before, acc.before_c, static_cast<double>(x.y));
+        fe_kahan_add(acc.before, acc.before_c, static_cast<double>(x.z));
+        fe_kahan_add(acc.before, acc.before_c, static_cast<double>(x.w));
         acc.before_abs += fabs(static_cast<double>(x.x));
         acc.before_abs += fabs(static_cast<double>(x.y));
         acc.before_abs += fabs(static_cast<double>(x.z));
@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(256) totals_f32(const float* __restrict__ v, s
     // The tail past the last float4 belongs to the block whose slice holds it (empty slices at the end hold nothing).
     for (size_t i = max(b0, b1 / 4 * 4) + threadIdx.x; i < b1; i += blockDim.x) {
         const double x = static_cast<double>(w[i]);
-        acc.before += x;
+        fe_kahan_add(acc.before, acc.before_c, x);
         acc.before_abs += fabs(x);
     }
     fe_acc_block(acc, scratch, partials + 4 * static_cast<size_t>(blockIdx.x), rec);

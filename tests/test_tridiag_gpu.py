@@ -100,12 +100,12 @@ def test_transposed_x_solve_matches_the_oracle(cuda):
 
 
 def test_solve_kernels_are_timed_alone(cuda):
-    """fe_law_time_stage: the Douglas law's x and y solves (its stages 1 and 2 after the stored explicit rate) each
-    timed by itself on a 256 x 128 x 64 lattice; the x solve is the warp-a-line kernel."""
+    """fe_law_time_stage: the Douglas law's x and y solves (its stages after the stored explicit rate) each timed by
+    itself on the calibration's lattice, 256 x 128 x 512 (65,536 x lines: 16,384 blocks of the warp-a-line kernel)."""
     from fieldcuda.solver import Solver
-    meta, init = start("heston_douglas.law", (64, 128, 256), 5)
+    meta, init = start("heston_douglas.law", (512, 128, 256), 5)
     text = open(os.path.join(ROOT, "tests", "laws", "heston_douglas.law")).read()
-    s = Solver(text, 256, 128, 64, 6.0 / 256, "heston_douglas.law")
+    s = Solver(text, 256, 128, 512, 6.0 / 256, "heston_douglas.law")
     for k, v in init.items():
         s.set_field(k, v)
     s.step(0.001)
