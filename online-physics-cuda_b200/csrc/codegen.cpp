@@ -354,15 +354,30 @@ private:
             static const char* sides[6][4] = {{"IN || x > 0", "x - 1", "y", "z"}, {"IN || x + 1 < NX", "x + 1", "y", "z"},
                 {"IN || y > 0", "x", "y - 1", "z"}, {"IN || y + 1 < NY", "x", "y + 1", "z"}, {"IN || z > 0", "x", "y", "z - 1"},
                 {"IN || z + 1 < NZ", "x", "y", "z + 1"}};
+            // A face's flux is antisymmetric to the bit: (b - a) = -(a - b) in IEEE arithmetic, and the harmonic mean is
+            // symmetric in its two conductivities. So the lower face of a cell (-x, -y, -z) is written as its lower
+            // neighbour's upper face, subtracted: acc - (c - nb) is acc + (nb - c) exactly (acc, a sum from +0, is never
+            // -0). The cells a lane computes side by side along x and the rows it computes along y then name the same
+            // difference twice, and the compiler computes it once (CudaCodegen.cpp:193-206 is the arithmetic kept).
+            static const bool lower[6] = {true, false, true, false, true, false};
             if (at(in.args[0]).shape == Shape::Scalar) {
-                // One k everywhere: the harmonic mean of a face is k itself (CudaCodegen.cpp:193-206).
+                // One k everywhere: the harmonic mean of a face is k itself.
                 f << " { const float c0 = " << a(1) << "; float acc = 0.f;\n";
-                for (const auto& s : sides) f << "    if (" << s[0] << ") acc += " << a(1, s[1], s[2], s[3]) << " - c0;\n";
+                for (int k = 0; k < 6; ++k) {
+                    const auto& s = sides[k];
+                    if (lower[k]) f << "    if (" << s[0] << ") acc -= c0 - " << a(1, s[1], s[2], s[3]) << ";\n";
+                    else f << "    if (" << s[0] << ") acc += " << a(1, s[1], s[2], s[3]) << " - c0;\n";
+                }
                 f << "    return fmaxf(" << a(0) << ", 0.f) * acc / (FE_H * FE_H); }\n";
             } else {
                 f << " { const float ka = " << a(0) << "; const float c0 = " << a(1) << "; float acc = 0.f;\n";
-                for (const auto& s : sides) {
-                    f << "    if (" << s[0] << ") acc += fe_face(ka, " << a(0, s[1], s[2], s[3]) << ", c0, " << a(1, s[1], s[2], s[3]) << ");\n";
+                for (int k = 0; k < 6; ++k) {
+                    const auto& s = sides[k];
+                    if (lower[k]) {
+                        f << "    if (" << s[0] << ") acc -= fe_face(" << a(0, s[1], s[2], s[3]) << ", ka, " << a(1, s[1], s[2], s[3]) << ", c0);\n";
+                    } else {
+                        f << "    if (" << s[0] << ") acc += fe_face(ka, " << a(0, s[1], s[2], s[3]) << ", c0, " << a(1, s[1], s[2], s[3]) << ");\n";
+                    }
                 }
                 f << "    return acc / (FE_H * FE_H); }\n";
             }

@@ -299,6 +299,7 @@ struct FeOutAcc {
     float pa, paa;  // this plane's fp32 partials of after and |after|
     float lo, hi;   // least and most value so far (NaN ignored)
     unsigned changed;
+    unsigned diff;  // this plane's cells' before ^ after, OR-ed (fe_out_plane folds it into changed)
 };
 
 __device__ __forceinline__ void fe_out_init(FeOutAcc& a)
@@ -307,11 +308,12 @@ __device__ __forceinline__ void fe_out_init(FeOutAcc& a)
     a.pa = 0.f; a.paa = 0.f;
     a.lo = __int_as_float(0x7f800000); a.hi = __int_as_float(0xff800000);
     a.changed = 0u;
+    a.diff = 0u;
 }
 
-// Four consecutive cells: their values before the pass (for the change flag) and after it. `mask` is all ones on an owned
-// plane and zero on a halo plane, whose sums the plane's end drops.
-__device__ __forceinline__ void fe_out_row4(FeOutAcc& a, const float* before, const float* after, bool range, unsigned mask)
+// Four consecutive cells: their values before the pass (for the change flag) and after it. A halo plane's sums and
+// change bits are dropped at the plane's end.
+__device__ __forceinline__ void fe_out_row4(FeOutAcc& a, const float* before, const float* after, bool range)
 {
     a.pa += (after[0] + after[1]) + (after[2] + after[3]);
     a.paa += (fabsf(after[0]) + fabsf(after[1])) + (fabsf(after[2]) + fabsf(after[3]));
@@ -319,10 +321,9 @@ __device__ __forceinline__ void fe_out_row4(FeOutAcc& a, const float* before, co
         a.lo = fminf(a.lo, fminf(fminf(after[0], after[1]), fminf(after[2], after[3])));
         a.hi = fmaxf(a.hi, fmaxf(fmaxf(after[0], after[1]), fmaxf(after[2], after[3])));
     }
-    a.changed |= (((__float_as_uint(before[0]) ^ __float_as_uint(after[0])) | (__float_as_uint(before[1]) ^ __float_as_uint(after[1])) |
-                      (__float_as_uint(before[2]) ^ __float_as_uint(after[2])) | (__float_as_uint(before[3]) ^ __float_as_uint(after[3]))) &
-                     mask) != 0u
-        ? 1u : 0u;
+    // One three-input logic op a cell ((b ^ a) | diff); the test against zero waits for the plane's end.
+#pragma unroll
+    for (int q = 0; q < 4; ++q) a.diff |= __float_as_uint(before[q]) ^ __float_as_uint(after[q]);
 }
 
 // Ends a plane: its partials into the FP64 totals. True when the plane may hold a bad cell (a bound past the declared
@@ -330,6 +331,8 @@ __device__ __forceinline__ void fe_out_row4(FeOutAcc& a, const float* before, co
 // range, so every later plane of the pass is read back too, and each bad cell is counted once, in its own plane.
 __device__ __forceinline__ bool fe_out_plane(FeOutAcc& a, float lo, float hi, bool range)
 {
+    a.changed |= a.diff != 0u ? 1u : 0u;
+    a.diff = 0u;
     const bool suspect = range && !(a.lo >= lo && a.hi <= hi && fabsf(a.pa) <= 3.0e38f);
     fe_kahan_add(a.after, a.after_c, static_cast<double>(a.pa));
     a.after_abs += static_cast<double>(a.paa);
@@ -691,7 +694,6 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         // Halo planes (another rank's) are computed like the rest; their contributions to the contracts are dropped.
         const bool own = !HALO || (z >= a.own_z0 && z < a.own_z1);
         const bool range_here = range && own;
-        const unsigned own_mask = own ? 0xffffffffu : 0u;
         FeSlabCtx<P> c;
         c.sm = fe_sm;
         c.x0 = x0;
@@ -733,7 +735,7 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
                 if (P::checked(j) && a.rec[j] != nullptr) {
                     const float bb[4] = {b[0][j], b[1][j], b[2][j], b[3][j]};
                     const float oo[4] = {o[0][j], o[1][j], o[2][j], o[3][j]};
-                    fe_out_row4(acc[j], bb, oo, range_here, own_mask);
+                    fe_out_row4(acc[j], bb, oo, range_here);
                 }
             }
         }
@@ -742,6 +744,7 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
             if (!own) {
                 acc[j].pa = 0.f;
                 acc[j].paa = 0.f;
+                acc[j].diff = 0u;
             } else if (P::checked(j) && a.rec[j] != nullptr && fe_out_plane(acc[j], a.lo[j], a.hi[j], range)) {
                 // Read this lane's cells of the plane back (its own stores, through L2) and tally the bad ones.
 #pragma unroll
