@@ -906,8 +906,22 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
                   << "::P>(a); }\n";
             }
         } else {
-            f << "extern \"C\" __global__ void __launch_bounds__(128) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_tridiag_yz_pass<"
-              << ns << "::P, " << axis << ">(a); }\n";
+            const int n = axis == 1 ? ny_ : nz_;
+            const int other = axis == 1 ? nz_ : ny_;
+            // Segments of M rows, K of them a line (at most 16: a block of 32 K threads holds 32 lines and keeps 4 M
+            // floats a thread in registers, so 512 threads at most).
+            const int m = n > 128 ? 16 : 8;
+            const int k = (n + m - 1) / m;
+            if (n >= 2 * m && k <= 16 && other <= 65535) {
+                L.tri_rows = m;
+                L.tri_segs = k;
+                f << "extern \"C\" __global__ void __launch_bounds__(" << 32 * k << ") " << L.kernel
+                  << "(const __grid_constant__ FePassArgs a) { fe_tridiag_yz_seg<" << ns << "::P, " << axis << ", " << m << ", " << k << ">(a); }\n";
+            } else {
+                L.tri_rows = 0;
+                f << "extern \"C\" __global__ void __launch_bounds__(128) " << L.kernel << "(const __grid_constant__ FePassArgs a) { fe_tridiag_yz_pass<"
+                  << ns << "::P, " << axis << ">(a); }\n";
+            }
         }
         out_ << f.str();
         return true;

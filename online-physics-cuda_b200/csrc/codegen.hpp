@@ -48,8 +48,10 @@ struct Launch {
     // Net: a `half` net op on the tensor cores (128 threads a CTA, persistent); at most this many CTAs an SM hold
     // tensor memory at once (the shared memory asked for keeps more from being resident).
     int per_sm = 0;
-    // TridiagX: rows a lane of the warp-a-line partition solve (0: the 32-lines-a-block Thomas pass).
+    // TridiagX: rows a lane of the warp-a-line partition solve (0: the 32-lines-a-block Thomas pass). TridiagYZ: rows
+    // a segment of the 32-lines-a-block partition solve, `tri_segs` segments a line (0: a thread a line).
     int tri_rows = 0;
+    int tri_segs = 0;
 };
 
 // The warp-a-line x solve: up to this many rows a lane (lines of up to 32 x this many cells), this many warps a block.

@@ -392,9 +392,16 @@ bool Engine::launch(const gen::Launch& L, float dt, int flags, FeCheck* const* r
         smem = L.smem;
         break;
     case gen::Launch::TridiagYZ: {
-        const unsigned long long lines = L.axis == 1 ? static_cast<unsigned long long>(nx_) * nz_ : static_cast<unsigned long long>(nx_) * ny_;
-        block = 128;
-        gx = static_cast<unsigned>((lines + 127) / 128);
+        if (L.tri_rows > 0) {
+            // 32 consecutive x a block, one block a (z of a y line | y of a z line), tri_segs segments a line.
+            gx = static_cast<unsigned>((nx_ + 31) / 32);
+            gy = static_cast<unsigned>(L.axis == 1 ? nz_ : ny_);
+            block = static_cast<unsigned>(32 * L.tri_segs);
+        } else {
+            const unsigned long long lines = L.axis == 1 ? static_cast<unsigned long long>(nx_) * nz_ : static_cast<unsigned long long>(nx_) * ny_;
+            block = 128;
+            gx = static_cast<unsigned>((lines + 127) / 128);
+        }
         break;
     }
     case gen::Launch::Reduce:

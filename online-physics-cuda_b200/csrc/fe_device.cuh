@@ -1127,6 +1127,106 @@ __device__ __forceinline__ void fe_tridiag_x_pass(const FePassArgs& a)
     }
 }
 
+// Tridiagonal solves along y or z by the partition method, 32 lines a block (32 consecutive x at one z, or one y), each
+// line cut into K segments of M rows: thread (k, line) = threadIdx.x = 32 k + line holds rows k M .. k M + M - 1, so
+// every load and store of a warp touches 32 consecutive x (coalesced). Each thread eliminates inside its rows (the
+// sweeps of fe_tri_line), leaving two rows that couple its first and last unknowns to the neighbouring segments'; those
+// 2 K rows a line go to shared memory, one thread a line solves them (Thomas), and every thread back-substitutes its
+// interior rows. Lines: NX x NZ (y) or NX x NY (z); the edge repeat folded at each line's ends, rows past the end the
+// identity. Reciprocals correctly rounded.
+template <class P, int AXIS, int M, int K>
+__device__ __forceinline__ void fe_tridiag_yz_seg(const FePassArgs& a)
+{
+    static_assert(M >= 2 && K >= 1 && K <= 16, "2 rows a segment at least, at most 16 segments");
+    __shared__ float red[32][8 * K + 1]; // per line: its 2 K reduced rows, (a, b, c, d) each
+    __shared__ float sol[32][2 * K + 1]; // per line: the segments' first and last unknowns
+    const int line = threadIdx.x & 31;
+    const int k = threadIdx.x >> 5;
+    const int n = AXIS == 1 ? P::NY : P::NZ;
+    const int x = blockIdx.x * 32 + line;
+    const int other = blockIdx.y; // the z of a y line, the y of a z line
+    const bool live = x < P::NX;
+    FePlainCtx<P> ctx;
+    ctx.src = a.src;
+    ctx.dt = a.dt;
+    float ra[M], rb[M], rc[M], rd[M];
+#pragma unroll
+    for (int r = 0; r < M; ++r) {
+        const int i = k * M + r;
+        float lo = 0.f, di = 1.f, up = 0.f, rhs = 0.f;
+        if (live && i < n) {
+            if (AXIS == 1) P::coef(ctx, x, i, other, lo, di, up, rhs);
+            else P::coef(ctx, x, other, i, lo, di, up, rhs);
+            if (i == 0) { di += lo; lo = 0.f; }
+            if (i + 1 == n) { di += up; up = 0.f; }
+        }
+        ra[r] = lo;
+        rb[r] = di;
+        rc[r] = up;
+        rd[r] = rhs;
+    }
+    // Down: the segment's last row in terms of its first unknown, itself and the next segment's first.
+    float al = ra[1], be = rb[1], de = rd[1];
+#pragma unroll
+    for (int r = 2; r < M; ++r) {
+        const float f = ra[r] * __frcp_rn(be);
+        al = -f * al;
+        be = rb[r] - f * rc[r - 1];
+        de = rd[r] - f * de;
+    }
+    // Up, in place: rb[r] becomes 1 / (row r's diagonal), rc[r] the coefficient of the segment's last unknown.
+    float diag0 = rb[M - 2];
+    rb[M - 2] = __frcp_rn(diag0);
+#pragma unroll
+    for (int r = M - 3; r >= 0; --r) {
+        const float g = rc[r] * rb[r + 1];
+        diag0 = rb[r] - g * ra[r + 1];
+        rc[r] = -g * rc[r + 1];
+        rd[r] = rd[r] - g * rd[r + 1];
+        rb[r] = __frcp_rn(diag0);
+    }
+    float* mine = &red[line][8 * k];
+    mine[0] = ra[0]; mine[1] = diag0; mine[2] = rc[0]; mine[3] = rd[0];
+    mine[4] = al; mine[5] = be; mine[6] = rc[M - 1]; mine[7] = de;
+    __syncthreads();
+    if (k == 0) {
+        // The line's 2 K reduced rows by Thomas, c' kept in place of the rows' c.
+        float* row = &red[line][0];
+        float cp = 0.f, dp = 0.f;
+        for (int j = 0; j < 2 * K; ++j) {
+            const float aj = row[4 * j], bj = row[4 * j + 1], cj = row[4 * j + 2], dj = row[4 * j + 3];
+            const float inv = __frcp_rn(bj - aj * cp);
+            cp = cj * inv;
+            dp = (dj - aj * dp) * inv;
+            row[4 * j + 2] = cp;
+            row[4 * j + 3] = dp;
+        }
+        float next = 0.f;
+        for (int j = 2 * K - 1; j >= 0; --j) {
+            next = row[4 * j + 3] - row[4 * j + 2] * next;
+            sol[line][j] = next;
+        }
+    }
+    __syncthreads();
+    const float first = sol[line][2 * k], last = sol[line][2 * k + 1];
+    float prev = first;
+    rd[0] = first;
+#pragma unroll
+    for (int r = 1; r < M - 1; ++r) {
+        prev = (rd[r] - ra[r] * prev - rc[r] * last) * rb[r];
+        rd[r] = prev;
+    }
+    rd[M - 1] = last;
+    if (!live) return;
+#pragma unroll
+    for (int r = 0; r < M; ++r) {
+        const int i = k * M + r;
+        if (i >= n) break;
+        const fe_u64 at = AXIS == 1 ? (static_cast<fe_u64>(other) * P::NY + i) * P::NX + x : (static_cast<fe_u64>(i) * P::NY + other) * P::NX + x;
+        a.out[0][at] = rd[r];
+    }
+}
+
 // Tridiagonal solves along y or z, a thread a line; consecutive threads take consecutive x, so every step of the
 // recurrence reads and writes whole rows (coalesced). c' goes to out[1] (scratch), d' and then the answer to out[0].
 template <class P, int AXIS>

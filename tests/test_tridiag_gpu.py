@@ -74,6 +74,60 @@ def test_x_solves_match_the_oracle(cuda, law, tol, nx):
     s2.close()
 
 
+YZ_SHAPES = [(3, 16, 40), (3, 64, 36), (2, 100, 33), (2, 128, 64), (2, 256, 40), (40, 20, 36), (130, 6, 32)]
+
+
+@pytest.mark.parametrize("shape", YZ_SHAPES, ids=str)
+@pytest.mark.parametrize("law,tol", [("implicit_yz.law", 2e-5), ("heston_douglas.law", 1e-4)], ids=["implicit_yz", "heston_douglas"])
+def test_yz_solves_match_the_oracle(cuda, law, tol, shape):
+    """y and z lines by the segmented partition solve (32 lines a block, each cut into segments of 8 or 16 rows; lines
+    of 16 to 256 rows, ragged ends padded with identity rows), or a thread a line where a line is too short to cut."""
+    nz, ny, nx = shape
+    if law.startswith("heston"):
+        meta, init = start(law, shape, sum(shape))
+    else:
+        rng = np.random.default_rng(sum(shape))
+        z, y, x = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        T = 1 + 0.5 * np.cos(0.3 * x + 0.2 * y) * np.sin(0.25 * z + 0.1) + 0.01 * rng.normal(size=shape)
+        meta, init = {"h": 1.0 / max(ny, nz), "dt": 0.001}, {"T": T.astype(np.float32)}
+    s, o = run_both(law, meta, init, shape)
+    for name in s.field_names:
+        if name not in o.fields:
+            continue
+        got = s.values(name).astype(np.float64)
+        want = o.fields[name].astype(np.float64)
+        scale = max(float(np.abs(want).max()), 1e-6)
+        assert float(np.abs(got - want).max()) <= tol * scale, (law, shape, name, float(np.abs(got - want).max()) / scale)
+    d = s.digest()
+    s.close()
+    s2, _ = run_both(law, meta, init, shape)
+    assert s2.digest() == d, "two runs differ"
+    s2.close()
+
+
+def test_transposed_yz_solves_match_the_oracle(cuda):
+    law = ("field A init 0 range -1e9 1e9\nfield B init 0 range -1e9 1e9\nterm t\n"
+           "  d A = tridiag_y_t(-0.2 * (1 + B), 1.6 + 0.1 * A, -0.3 + 0.05 * B, A) + tridiag_z_t(-0.1, 1.3 + 0.1 * B, -0.25 * A, B) - A\n")
+    from fieldcuda import solver as sv
+    from fieldcuda.solver import Solver
+    from oracle import law_cpu
+    ir = json.loads(sv.ir_json(law))
+    rng = np.random.default_rng(4)
+    for shape in ((40, 100, 33), (3, 256, 32)):
+        nz, ny, nx = shape
+        init = {"A": rng.uniform(0, 1, shape).astype(np.float32), "B": rng.uniform(0, 1, shape).astype(np.float32)}
+        s = Solver(law, nx, ny, nz, 0.5)
+        o = law_cpu.Solver(law_cpu.Law(ir), shape, 0.5)
+        for k, v in init.items():
+            s.set_field(k, v)
+            o.fields[k] = v.copy()
+        s.step(0.01)
+        o.step(0.01)
+        got, want = s.values("A").astype(np.float64), o.fields["A"].astype(np.float64)
+        assert float(np.abs(got - want).max()) <= 2e-5 * float(np.abs(want).max()), shape
+        s.close()
+
+
 def test_transposed_x_solve_matches_the_oracle(cuda):
     """tridiag_x_t (the adjoint laws' solve): below the diagonal the previous cell's `up`, above it the next cell's
     `lo`, through the same warp-a-line kernel."""
