@@ -910,7 +910,7 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
             const int other = axis == 1 ? nz_ : ny_;
             // Segments of M rows, K of them a line (at most 16: a block of 32 K threads holds 32 lines and keeps 4 M
             // floats a thread in registers, so 512 threads at most).
-            const int m = n > 128 ? 16 : 8;
+            const int m = n >= 128 ? 16 : 8;
             const int k = (n + m - 1) / m;
             if (n >= 2 * m && k <= 16 && other <= 65535) {
                 L.tri_rows = m;

@@ -265,15 +265,18 @@ CUfunction Engine::function(const std::string& name, unsigned smem, std::string&
 int Engine::zchunk_for(const gen::Launch& L, bool slab) const
 {
     // Several waves of CTAs (a short last wave wastes little), and chunks long enough that the z halo is a small part of
-    // what is read (2 RZ planes of every 32 RZ) — but never so long that the grid falls under two waves: on a small
-    // lattice the halo re-reads come from L2, an idle SM is lost for good.
+    // what is read (2 RZ planes of every 32 RZ) — but never so long that the grid falls under two waves of resident
+    // CTAs: on a small lattice the halo re-reads come from L2, an idle SM is lost for good.
     const long long tiles = slab ? static_cast<long long>((nx_ + 127) / 128) * ((ny_ + L.ty - 1) / L.ty)
                                  : static_cast<long long>((nx_ + 31) / 32) * ((ny_ + 7) / 8);
     const long long want = static_cast<long long>(sms_) * (slab ? 12 : 16);
     const long long chunks = std::max<long long>(1, (want + tiles - 1) / tiles);
     int zchunk = static_cast<int>((nz_ + chunks - 1) / chunks);
     if (L.rz > 0) {
-        const long long two_waves = std::max<long long>(1, static_cast<long long>(nz_) * tiles / (2LL * sms_));
+        // A wave is every SM's resident CTAs: for a slab pass as many as its shared memory lets in (the 227 KB an SM
+        // hands out, 2 KB of it for the static part a CTA), at most 8.
+        const long long per_sm = slab ? std::max<long long>(1, std::min<long long>(8, (227LL * 1024) / (static_cast<long long>(L.smem) + 2048))) : 8;
+        const long long two_waves = std::max<long long>(1, static_cast<long long>(nz_) * tiles / (2LL * sms_ * per_sm));
         zchunk = std::max(zchunk, static_cast<int>(std::min<long long>({static_cast<long long>(nz_), 32LL * L.rz, two_waves})));
     }
     return std::max(1, zchunk);
