@@ -523,6 +523,12 @@ __device__ __forceinline__ void fe_acc_finish(const double* partials, int blocks
 // which outputs carry contracts (checked(j)), and `cell(ctx, x, y, z, out, before)`, which evaluates every output of the
 // pass at one cell.
 
+// A compile-time flag passed by value, for the generic lambdas of the pass skeletons.
+template <bool B>
+struct FeFlag {
+    static constexpr bool value = B;
+};
+
 // Shared-memory reads of the staged sources: ld<k>(X, Y, Z) is source k at lattice cell (X, Y, Z), which the pass's
 // halos guarantee lies in the staged box.
 template <class P>
@@ -685,6 +691,10 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         if (y < P::NY && x < P::NX) live |= 1u << r;
         if (y - P::RYT >= 0 && y + P::RYT < P::NY) yin |= 1u << r;
     }
+    constexpr unsigned all_rows = (1u << P::R) - 1u;
+    bool track[P::NOUT];
+#pragma unroll
+    for (int j = 0; j < P::NOUT; ++j) track[j] = P::checked(j) && a.rec[j] != nullptr;
     const bool range = (a.flags & FE_PASS_RANGE) != 0;
     const fe_u64 row0 = static_cast<fe_u64>(P::NX) * static_cast<fe_u64>(y0 + warp * P::R) + static_cast<fe_u64>(x);
     // The ring stage of plane z, stepped with z; planes whose z reach stays in the lattice take their neighbours'
@@ -714,29 +724,37 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         }
         const bool plane_in = xin && z - P::RZT >= 0 && z + P::RZT < P::NZ;
         const fe_u64 plane0 = static_cast<fe_u64>(P::NX) * static_cast<fe_u64>(P::NY) * static_cast<fe_u64>(z) + row0;
-#pragma unroll
-        for (int r = 0; r < P::R; ++r) {
-            if (ragged && !((live >> r) & 1u)) continue;
+        // One row of four cells, clamp-free (IN) or clamped. The stores name the global space, so the compiler may
+        // move the next row's shared-memory loads above them.
+        auto row = [&](int r, auto in) {
+            constexpr bool IN = decltype(in)::value;
             const int y = y0 + warp * P::R + r;
             float o[4][P::NOUT];
             float b[4][P::NOUT];
-            // Four cells whose whole reach is inside the lattice take the clamp-free code; the rest the clamped one.
-            if (plane_in && ((yin >> r) & 1u)) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) P::template cell<true>(c, x + q, y, z, o[q], b[q]);
-            } else {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) P::template cell<false>(c, x + q, y, z, o[q], b[q]);
-            }
+            for (int q = 0; q < 4; ++q) P::template cell<IN>(c, x + q, y, z, o[q], b[q]);
             const fe_u64 at = plane0 + static_cast<fe_u64>(r) * P::NX;
 #pragma unroll
             for (int j = 0; j < P::NOUT; ++j) {
-                *reinterpret_cast<float4*>(a.out[j] + at) = make_float4(o[0][j], o[1][j], o[2][j], o[3][j]);
-                if (P::checked(j) && a.rec[j] != nullptr) {
+                __stwb(reinterpret_cast<float4*>(a.out[j] + at), make_float4(o[0][j], o[1][j], o[2][j], o[3][j]));
+                if (track[j]) {
                     const float bb[4] = {b[0][j], b[1][j], b[2][j], b[3][j]};
                     const float oo[4] = {o[0][j], o[1][j], o[2][j], o[3][j]};
                     fe_out_row4(acc[j], bb, oo, range_here);
                 }
+            }
+        };
+        if (plane_in && yin == all_rows && (!ragged || live == all_rows)) {
+            // The tile's whole plane is inside the lattice with its reach: its R rows are one branch-free block.
+#pragma unroll
+            for (int r = 0; r < P::R; ++r) row(r, FeFlag<true>{});
+        } else {
+#pragma unroll
+            for (int r = 0; r < P::R; ++r) {
+                if (ragged && !((live >> r) & 1u)) continue;
+                // Four cells whose whole reach is inside the lattice take the clamp-free code; the rest the clamped one.
+                if (plane_in && ((yin >> r) & 1u)) row(r, FeFlag<true>{});
+                else row(r, FeFlag<false>{});
             }
         }
 #pragma unroll

@@ -33,10 +33,9 @@ __global__ void __launch_bounds__(256) totals_f32(const float* __restrict__ v, s
 #pragma unroll 4
     for (size_t i = b0 / 4 + threadIdx.x; i < b1 / 4; i += blockDim.x) {
         const float4 x = __ldg(w4 + i);
-        fe_kahan_add(acc.before, acc.before_c, static_cast<double>(x.x));
-        fe_kahan_add(acc.before, acc.before_c, static_cast<double>(x.y));
-        fe_kahan_add(acc.before, acc.before_c, static_cast<double>(x.z));
-        fe_kahan_add(acc.before, acc.before_c, static_cast<double>(x.w));
+        // Four floats summed in FP64 are exact unless their exponents span more than 29 bits; the group then goes
+        // into the compensated total.
+        fe_kahan_add(acc.before, acc.before_c, (static_cast<double>(x.x) + static_cast<double>(x.y)) + (static_cast<double>(x.z) + static_cast<double>(x.w)));
         acc.before_abs += fabs(static_cast<double>(x.x));
         acc.before_abs += fabs(static_cast<double>(x.y));
         acc.before_abs += fabs(static_cast<double>(x.z));

@@ -91,6 +91,31 @@ def test_contracts_fused(cuda):
         assert (rec2.before, rec2.before_abs, rec2.after) == (rec.before, rec.before_abs, rec.after)
 
 
+def test_totals_are_compensated(cuda):
+    """Planes alternating +1e20, 1, -1e20, 1 (each constant, k = 0: nothing moves), four planes a z-chunk, so every
+    thread's run of planes cancels: the exact total is the 1-planes' cell count. Plain FP64 accumulation across a
+    thread's planes loses each 1 added next to 1e20 (its ulp there is 2^14), half of them; the compensated sum (Neumaier
+    from the plane partials on) keeps them, in every kernel variant. Each level of the fixed tree is compensated by
+    itself and hands its sum on as one double, so the guarantee is the sum of each level's rounding, not cancellation
+    across blocks: the case keeps the large values' cancellation inside a thread."""
+    import torch
+    from fieldcuda import kernels, _lib
+    nz, ny, nx = 16, 24, 128
+    T0 = np.empty((nz, ny, nx), np.float32)
+    for z in range(nz):
+        T0[z] = (1e20 if z % 4 == 0 else -1e20) if z % 2 == 0 else 1.0
+    exact = float(nx * ny * (nz // 2))
+    for variant in (-1, 0, 1):
+        a = torch.from_numpy(T0).cuda()
+        b = torch.empty_like(a)
+        ws = kernels.heat7_workspace(T0.shape, variant, 4)
+        kernels.check_reset(ws)
+        kernels.heat7_step(a, b, 0.0, 0.1, 0.001, lo=-1e30, hi=1e30, variant=variant, zchunk=4,
+                           check=_lib.FE_HEAT7_BEFORE | _lib.FE_HEAT7_AFTER, workspace=ws)
+        rec = kernels.check_read(ws)
+        assert rec.before == exact and rec.after == exact, (variant, rec.before, rec.after, exact)
+
+
 def test_not_finite_is_counted(cuda):
     import torch
     from fieldcuda import kernels, _lib
