@@ -1,6 +1,7 @@
 #include "codegen.hpp"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <functional>
@@ -60,6 +61,38 @@ Radius axis_radius(const Inst& in)
     case Op::Flux: return {1, 1, 1};
     case Op::LDiffuse: return {2, 2, 2};
     default: return {};
+    }
+}
+
+// The offsets (dx, dy, dz) at which an op reads its arguments, relative to its own cell: the exact points of the
+// stencils, the whole box where the points depend on values (spread, topple) or run over a range (the transposed
+// shifts), and the cell itself for the pointwise ops.
+void read_points(const Inst& in, std::vector<std::array<int, 3>>& pts)
+{
+    pts.clear();
+    auto box = [&](int rx, int ry, int rz) {
+        for (int dz = -rz; dz <= rz; ++dz)
+            for (int dy = -ry; dy <= ry; ++dy)
+                for (int dx = -rx; dx <= rx; ++dx) pts.push_back({dx, dy, dz});
+    };
+    auto star = [&](bool x, bool y, bool z) {
+        pts.push_back({0, 0, 0});
+        if (x) pts.insert(pts.end(), {{-1, 0, 0}, {1, 0, 0}});
+        if (y) pts.insert(pts.end(), {{0, -1, 0}, {0, 1, 0}});
+        if (z) pts.insert(pts.end(), {{0, 0, -1}, {0, 0, 1}});
+    };
+    switch (in.op) {
+    case Op::Shift: pts.push_back({in.offset[0], in.offset[1], in.offset[2]}); break;
+    case Op::ShiftT: box(std::abs(in.offset[0]), std::abs(in.offset[1]), std::abs(in.offset[2])); break;
+    case Op::Lap: case Op::Diffuse: case Op::Adv: case Op::Flux: star(true, true, true); break;
+    case Op::Gx: case Op::GxT: star(true, false, false); break;
+    case Op::Gy: case Op::GyT: star(false, true, false); break;
+    case Op::Gz: case Op::GzT: case Op::Fall: star(false, false, true); break;
+    case Op::Spread: box(1, 1, 0); break;
+    default: {
+        const Radius r = axis_radius(in);
+        box(r.x, r.y, r.z);
+    }
     }
 }
 
@@ -196,6 +229,12 @@ private:
         std::vector<Radius> reach;            // per source
         std::set<int> own_stages;             // stages whose bodies this pass computes
         std::set<std::pair<int, std::tuple<int, int, int>>> seen;
+        // The plane carry: per source, whether it is read below the cell's plane, and whether any such read is other
+        // than the cell's own column one plane down; cslot the carry slot of each source (-1: none).
+        std::set<std::pair<int, std::tuple<int, int, int>>> seen_points;
+        std::vector<char> below, below_off;
+        std::vector<int> cslot;
+        bool zcarry = false;
     };
 
     int source_index(PassBuild& pb, Buf buf)
@@ -205,7 +244,58 @@ private:
         }
         pb.sources.push_back(Source{buf});
         pb.reach.push_back({});
+        pb.below.push_back(0);
+        pb.below_off.push_back(0);
         return static_cast<int>(pb.sources.size()) - 1;
+    }
+
+    // The same closure as walk(), with signed offsets: which sources are read below the cell's plane, and whether each
+    // such read is the cell's own column one plane down (what the plane carry can serve).
+    void walk_points(PassBuild& pb, int id, int dx, int dy, int dz, bool body)
+    {
+        const Inst& in = at(id);
+        if (!pb.seen_points.insert({id * 2 + (body ? 1 : 0), {dx, dy, dz}}).second) return;
+        const bool stored = m_.is_stage(id) || in.global;
+        int k = -1;
+        if (!body && stored) {
+            if (in.shape == Shape::Scalar) return;
+            k = source_index(pb, Buf{Buf::Slot, plan_.slot_of[static_cast<std::size_t>(id)]});
+        } else if (in.op == Op::Field) {
+            k = source_index(pb, Buf{Buf::FieldNow, in.index});
+        }
+        if (k >= 0) {
+            if (dz < 0) {
+                pb.below[static_cast<std::size_t>(k)] = 1;
+                if (dz != -1 || dx != 0 || dy != 0) pb.below_off[static_cast<std::size_t>(k)] = 1;
+            }
+            return;
+        }
+        std::vector<std::array<int, 3>> pts;
+        read_points(in, pts);
+        for (const auto& p : pts) {
+            for (const int arg : in.args) walk_points(pb, arg, dx + p[0], dy + p[1], dz + p[2], false);
+        }
+    }
+
+    // The plane carry applies when the pass reads one plane each way (RZ = 1), every read below the plane is the cell's
+    // own column, and at most two sources need carrying (their cells of one plane live in registers).
+    void plan_carry(PassBuild& pb)
+    {
+        pb.cslot.assign(pb.sources.size(), -1);
+        pb.zcarry = false;
+        int rz = 0;
+        for (const Radius& r : pb.reach) rz = std::max(rz, r.z);
+        if (rz != 1) return;
+        int n = 0;
+        for (std::size_t k = 0; k < pb.sources.size(); ++k) {
+            if (pb.below_off[k]) return;
+            if (pb.below[k]) pb.cslot[k] = n++;
+        }
+        if (n == 0 || n > 2) {
+            pb.cslot.assign(pb.sources.size(), -1);
+            return;
+        }
+        pb.zcarry = true;
     }
 
     // Walks a value's inlined closure with the offset it is read at, growing the sources' reach. `body`: evaluate this
@@ -626,6 +716,20 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
         fn("pl", pl);
         fn("base", base);
         f << "    static constexpr unsigned BYTES = " << bytes << "u;\n";
+        {
+            int ncarry = 0;
+            std::vector<int> cs;
+            for (std::size_t k = 0; k < pb.sources.size(); ++k) {
+                const int v = pb.zcarry && k < pb.cslot.size() ? pb.cslot[k] : -1;
+                cs.push_back(v);
+                ncarry = std::max(ncarry, v + 1);
+            }
+            f << "    static constexpr bool ZCARRY = " << (pb.zcarry ? "true" : "false") << ";\n"
+              << "    static constexpr int NCARRY = " << ncarry << ";\n"
+              << "    static __device__ __forceinline__ constexpr int cslot(int k) { ";
+            for (std::size_t k = 0; k < cs.size(); ++k) f << "if (k == " << k << ") return " << cs[k] << "; ";
+            f << "return -1; }\n";
+        }
         // The pass's true reach along each axis (unrounded): a cell this far from every face is interior (IN).
         int rxt = 0, ryt = 0, rzt = 0;
         for (const Radius& r : pb.reach) {
@@ -660,8 +764,10 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
         // 3.09; 8-row tiles 3.2 whatever the ring), so the shallowest ring of at least 4 stages comes first, 16-row
         // tiles before 8, under budgets that leave room for 3, then 2, then 1 CTA an SM. A pass that reads no other
         // plane (RZ = 0) starts at 2 stages: the explicit Heston gather (7 sources, 512 x 256) takes 0.39 ms a substep
-        // on 128 planes with 2 stages against 0.65 with 4, which leave room for one CTA an SM only.
-        const int shallowest = rz == 0 ? 2 : std::max(4, 2 * rz + 2);
+        // on 128 planes with 2 stages against 0.65 with 4, which leave room for one CTA an SM only. With the plane carry
+        // the ring holds planes z and z + 1 and the one being fetched: the 512^3 heat gather (32-row tiles, 76 registers:
+        // 3 CTAs an SM) 4.84 TB/s with 3 stages, 4.77 with 4; forced to 64 registers for 4 CTAs an SM it spills, 4.37.
+        const int shallowest = rz == 0 ? 2 : (pb.zcarry ? rz + 2 : std::max(4, 2 * rz + 2));
         // First, 32-row tiles when they leave room for 3 CTAs an SM (a warp then computes 4 rows of a plane, so the
         // per-plane waits, barrier and ring bookkeeping are shared by 16 cells a lane): the 512^3 heat gather, 16-row
         // tiles 4.15 TB/s (5 CTAs an SM), 24 rows 4.10, 32 rows 4.41 (3 CTAs), 32 rows with 5 stages 4.02, 40 rows 3.34.
@@ -767,6 +873,8 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
         }
         const bool bodies = outs.front().kind == PassOut::StageBody;
         for (const int r : roots) walk(pb, r, Radius{}, bodies);
+        for (const int r : roots) walk_points(pb, r, 0, 0, 0, bodies);
+        plan_carry(pb);
         std::ostringstream f;
         const std::string ns = "fe_" + tag;
         f << "namespace " << ns << " {\n";
@@ -790,6 +898,7 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
         if (!L.slab) {
             L.ty = 16;
             L.nst = 4;
+            pb.zcarry = false;
         }
         emit_traits(f, pb, L, static_cast<int>(outs.size()), checked);
         f << "    static constexpr bool XFILL = " << (xfill_safe(roots, bodies) ? "true" : "false") << ";\n";

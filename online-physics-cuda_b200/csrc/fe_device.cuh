@@ -531,12 +531,19 @@ struct FeFlag {
 
 // Shared-memory reads of the staged sources: ld<k>(X, Y, Z) is source k at lattice cell (X, Y, Z), which the pass's
 // halos guarantee lies in the staged box.
+//
+// Plane carry (P::ZCARRY, passes with RZ = 1 whose every read below the cell's plane is the cell's own column, one
+// plane down): a source with such reads (P::cslot(k) >= 0) keeps the lane's own cells of plane z - 1 (R rows of 4) in
+// registers, captured while plane z - 1 was computed. The ring then holds planes z and z + 1 only, and a plane's stage
+// is handed back as soon as the plane is computed.
 template <class P>
 struct FeSlabCtx {
     const float* sm;
     int slots[2 * P::RZ + 1]; // the ring stage of plane z + d at slots[d + RZ]
     int x0, y0, z;
+    int xl, yl;               // the lane's first column and the warp's first row
     float dt;
+    float carry[P::NCARRY > 0 ? P::NCARRY : 1][P::R][4];
     // The stage of plane Z (|Z - z| <= RZ): a chain of selects, so the table stays in registers whatever Z is.
     __device__ __forceinline__ int stage(int Z) const
     {
@@ -546,9 +553,24 @@ struct FeSlabCtx {
         for (int i = 1; i < 2 * P::RZ + 1; ++i) s = d == i ? slots[i] : s;
         return s;
     }
+    // A carried cell by its row and column within the lane's: constants in the clamp-free code, a chain of selects
+    // (no indexed register array) where clamps leave them to run time.
+    __device__ __forceinline__ float pick(const float (&cr)[P::R][4], int dr, int dq) const
+    {
+        float v = cr[0][0];
+#pragma unroll
+        for (int r = 0; r < P::R; ++r) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) v = (dr == r && dq == q) ? cr[r][q] : v;
+        }
+        return v;
+    }
     template <int k>
     __device__ __forceinline__ float ld(int X, int Y, int Z) const
     {
+        if constexpr (P::ZCARRY && P::cslot(k) >= 0) {
+            if (Z < z) return pick(carry[P::cslot(k)], Y - yl, X - xl);
+        }
         return sm[P::base(k) + stage(Z) * P::pl(k) + (Y - y0 + P::ry(k)) * P::px(k) + (X - x0 + P::ax(k))];
     }
 };
@@ -614,10 +636,24 @@ __device__ __forceinline__ void fe_pass_contracts(FeOutAcc* acc, double* scratch
     }
 }
 
+// The carried sources' cells of row r of plane z (the lane's 4 columns), into the plane carry (P::ZCARRY).
+template <class P, int K = 0>
+__device__ __forceinline__ void fe_carry_row(FeSlabCtx<P>& c, int r, int x, int y, int z)
+{
+    if constexpr (K < P::NSRC) {
+        if constexpr (P::cslot(K) >= 0) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) c.carry[P::cslot(K)][r][q] = c.template ld<K>(x + q, y, z);
+        }
+        fe_carry_row<P, K + 1>(c, r, x, y, z);
+    }
+}
+
 // The TMA z-marching pass: a CTA owns a 128 x TY column and marches a chunk of z-planes; every source's plane (with its
-// halo) comes into a ring of NST stages by one TMA load each, NST - 2 RZ - 1 planes ahead; one mbarrier a stage counts
-// the bytes of all sources. A lane computes 4 consecutive cells on R rows and stores them as float4. HALO: the handle
-// holds halo planes another rank owns (a lattice split in z-slabs), left out of the contracts.
+// halo) comes into a ring of NST stages by one TMA load each, NST - 2 RZ - 1 planes ahead (NST - RZ - 1 with the plane
+// carry); one mbarrier a stage counts the bytes of all sources. A lane computes 4 consecutive cells on R rows and stores
+// them as float4. HALO: the handle holds halo planes another rank owns (a lattice split in z-slabs), left out of the
+// contracts.
 template <class P, bool HALO = false>
 __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
 {
@@ -625,7 +661,9 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
     __shared__ __align__(8) fe_u64 bar[P::NST];
     __shared__ double scratch[4 * P::W];
     __shared__ unsigned fails[P::NOUT][3];
-    static_assert(P::NST >= 2 * P::RZ + 2, "the ring holds 2 RZ + 1 planes and the one being fetched");
+    static_assert(P::NST >= (P::ZCARRY ? P::RZ + 2 : 2 * P::RZ + 2),
+        "the ring holds the planes a z reads from shared memory and the one being fetched");
+    static_assert(!P::ZCARRY || P::RZ == 1, "the plane carry holds one plane");
     const int x0 = blockIdx.x * 128;
     const int y0 = blockIdx.y * (P::W * P::R);
     const int zb = blockIdx.z * a.zchunk;
@@ -676,8 +714,34 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         }
     };
     if (zb < ze) wait_upto(min(zb + P::RZ, P::NZ - 1) - zlo);
-    bool failed = __syncthreads_or(ok ? 0 : 1) != 0;
     const int x = x0 + 4 * lane;
+    FeSlabCtx<P> c;
+    c.sm = fe_sm;
+    c.x0 = x0;
+    c.y0 = y0;
+    c.xl = x;
+    c.yl = y0 + warp * P::R;
+    c.dt = a.dt;
+    // With the plane carry, a chunk that starts above the lattice's first plane takes plane zb - 1 (ring stage 0, which
+    // this thread waited for) into it; the stage goes back to the ring after the barrier.
+    const bool carry_in = P::ZCARRY && zb > zlo;
+    if (carry_in && ok) {
+        c.z = zlo;
+#pragma unroll
+        for (int d = 0; d < 2 * P::RZ + 1; ++d) c.slots[d] = 0;
+#pragma unroll
+        for (int r = 0; r < P::R; ++r) fe_carry_row<P>(c, r, x, y0 + warp * P::R + r, zlo);
+    }
+    bool failed = __syncthreads_or(ok ? 0 : 1) != 0;
+    int released = 0; // thread 0's next plane to hand back to the ring
+    if (carry_in && threadIdx.x == 0 && !failed) {
+        if (P::NST < nplanes) {
+            if (edge) fe_fence_proxy_async();
+            issue(P::NST);
+            issued = P::NST + 1;
+        }
+        released = 1;
+    }
     // With the x edge carried by the halo, whether a row's cells are interior depends only on the row and the plane, so
     // a warp takes one path. Which of this warp's rows lie in the lattice, and which have their whole y reach inside
     // it, are fixed for the pass.
@@ -692,9 +756,6 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         if (y - P::RYT >= 0 && y + P::RYT < P::NY) yin |= 1u << r;
     }
     constexpr unsigned all_rows = (1u << P::R) - 1u;
-    bool track[P::NOUT];
-#pragma unroll
-    for (int j = 0; j < P::NOUT; ++j) track[j] = P::checked(j) && a.rec[j] != nullptr;
     const bool range = (a.flags & FE_PASS_RANGE) != 0;
     const fe_u64 row0 = static_cast<fe_u64>(P::NX) * static_cast<fe_u64>(y0 + warp * P::R) + static_cast<fe_u64>(x);
     // The ring stage of plane z, stepped with z; planes whose z reach stays in the lattice take their neighbours'
@@ -704,12 +765,7 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         // Halo planes (another rank's) are computed like the rest; their contributions to the contracts are dropped.
         const bool own = !HALO || (z >= a.own_z0 && z < a.own_z1);
         const bool range_here = range && own;
-        FeSlabCtx<P> c;
-        c.sm = fe_sm;
-        c.x0 = x0;
-        c.y0 = y0;
         c.z = z;
-        c.dt = a.dt;
         if (z - P::RZ >= 0 && z + P::RZ < P::NZ) {
 #pragma unroll
             for (int d = -P::RZ; d <= P::RZ; ++d) {
@@ -725,7 +781,9 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         const bool plane_in = xin && z - P::RZT >= 0 && z + P::RZT < P::NZ;
         const fe_u64 plane0 = static_cast<fe_u64>(P::NX) * static_cast<fe_u64>(P::NY) * static_cast<fe_u64>(z) + row0;
         // One row of four cells, clamp-free (IN) or clamped. The stores name the global space, so the compiler may
-        // move the next row's shared-memory loads above them.
+        // move the next row's shared-memory loads above them. A checked output's sums, bounds and change bits are taken
+        // whether or not the launch asked for them (no branch a row): a launch without a record never reads them, and
+        // one without the range test has its bounds emptied before they are folded (a halo plane's stay out by test).
         auto row = [&](int r, auto in) {
             constexpr bool IN = decltype(in)::value;
             const int y = y0 + warp * P::R + r;
@@ -733,14 +791,16 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
             float b[4][P::NOUT];
 #pragma unroll
             for (int q = 0; q < 4; ++q) P::template cell<IN>(c, x + q, y, z, o[q], b[q]);
+            // The row's cells of plane z replace those of plane z - 1 in the carry (read above, by this row only).
+            if constexpr (P::ZCARRY) fe_carry_row<P>(c, r, x, y, z);
             const fe_u64 at = plane0 + static_cast<fe_u64>(r) * P::NX;
 #pragma unroll
             for (int j = 0; j < P::NOUT; ++j) {
                 __stwb(reinterpret_cast<float4*>(a.out[j] + at), make_float4(o[0][j], o[1][j], o[2][j], o[3][j]));
-                if (track[j]) {
+                if (P::checked(j)) {
                     const float bb[4] = {b[0][j], b[1][j], b[2][j], b[3][j]};
                     const float oo[4] = {o[0][j], o[1][j], o[2][j], o[3][j]};
-                    fe_out_row4(acc[j], bb, oo, range_here);
+                    fe_out_row4(acc[j], bb, oo, HALO ? range_here : true);
                 }
             }
         };
@@ -780,11 +840,17 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
         }
         if (z + 1 < ze) wait_upto(min(z + 1 + P::RZ, P::NZ - 1) - zlo);
         failed = __syncthreads_or(ok ? 0 : 1) != 0;
-        const int release = z - P::RZ - zlo;
-        if (threadIdx.x == 0 && !failed && release >= 0 && release + P::NST < nplanes) {
-            fe_fence_proxy_async();
-            issue(release + P::NST);
-            issued = release + P::NST + 1;
+        // The planes no later z reads from shared memory go back to the ring: plane z - RZ, or plane z itself with the
+        // carry. Their last readers passed the barrier above; only the x-edge fill wrote them through the generic proxy,
+        // and those writes must be ordered before the TMA overwrites them.
+        if (threadIdx.x == 0 && !failed) {
+            const int upto = z - (P::ZCARRY ? 0 : P::RZ) - zlo;
+            if (released <= upto && released + P::NST < nplanes && edge) fe_fence_proxy_async();
+            while (released <= upto && released + P::NST < nplanes) {
+                issue(released + P::NST);
+                issued = released + P::NST + 1;
+                ++released;
+            }
         }
         if (++sz == P::NST) sz = 0;
     }
@@ -794,6 +860,13 @@ __device__ __forceinline__ void fe_slab_pass(const FePassArgs& a)
             for (int j = 0; j < issued; ++j) fe_mbar_wait(&bar[j % P::NST], static_cast<unsigned>((j / P::NST) & 1), 1u << 16);
         }
         return;
+    }
+    if (!range) {
+#pragma unroll
+        for (int j = 0; j < P::NOUT; ++j) {
+            acc[j].lo = __int_as_float(0x7f800000);
+            acc[j].hi = __int_as_float(0xff800000);
+        }
     }
     fe_pass_contracts<P>(acc, scratch, fails, a);
 }
