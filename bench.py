@@ -1132,8 +1132,8 @@ def run_ours(args, world, rank, local):
                    "handwritten_kernel_gbs": BYTES_PER_CELL * cells / (hand_ms * 1e-3) / 1e9},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of the same pass at "
-                     "512^3, copied from profiles/heat_gather_512.md (an ncu capture of its 16-row-tile shape; the traffic "
-                     "does not depend on the tile), not measured in this run",
+                     "512^3, copied from profiles/heat_gather_512.md (an ncu capture of the same pass; the traffic does "
+                     "not depend on the tile or the chunk length beyond the z halo), not measured in this run",
                      "kernel": "generated gather pass fe_pass_t0g (8 B/cell)",
                      "peak_source": f"{peak_kind} copy (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                      "copy_same_run_gbs": copy_gbs},

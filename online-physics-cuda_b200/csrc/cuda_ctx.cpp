@@ -78,7 +78,8 @@ const Driver& driver()
         const bool all = entry("cuTensorMapEncodeTiled", d.tensorMapEncodeTiled, why) && entry("cuModuleLoadData", d.moduleLoadData, why) &&
             entry("cuModuleUnload", d.moduleUnload, why) && entry("cuModuleGetFunction", d.moduleGetFunction, why) &&
             entry("cuLaunchKernel", d.launchKernel, why) && entry("cuFuncSetAttribute", d.funcSetAttribute, why) &&
-            entry("cuGetErrorString", d.getErrorString, why) && entry("cuModuleGetGlobal", d.moduleGetGlobal, why);
+            entry("cuGetErrorString", d.getErrorString, why) && entry("cuModuleGetGlobal", d.moduleGetGlobal, why) &&
+            entry("cuOccupancyMaxActiveBlocksPerMultiprocessor", d.occupancyMaxActiveBlocksPerMultiprocessor, why);
         if (!all) {
             d.why = why;
             return;

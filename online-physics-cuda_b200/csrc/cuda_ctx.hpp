@@ -29,6 +29,7 @@ struct Driver {
     CUresult (*funcSetAttribute)(CUfunction, CUfunction_attribute, int) = nullptr;
     CUresult (*getErrorString)(CUresult, const char**) = nullptr;
     CUresult (*moduleGetGlobal)(CUdeviceptr*, size_t*, CUmodule, const char*) = nullptr;
+    CUresult (*occupancyMaxActiveBlocksPerMultiprocessor)(int*, CUfunction, int, size_t) = nullptr;
 };
 
 // The driver entry points, looked up once (thread-safe). `ok` is false, with the reason, without a usable driver.

@@ -148,7 +148,9 @@ private:
     bool buffer(const gen::Buf& b, float*& out) const;
     bool map_for(const float* base, int bx, int by, FeTensorMap& out, std::string& why);
     CUfunction function(const std::string& name, unsigned smem, std::string& why);
-    int zchunk_for(const gen::Launch& L, bool slab) const;
+    int zchunk_for(const gen::Launch& L, bool slab);
+    // CTAs of a slab pass an SM holds at once (its shared memory and its registers both counted), cached by kernel.
+    int resident(const gen::Launch& L);
     bool run_program(int index, const ir::Program& p, const gen::ProgramPlan& pp, double dt, bool respect, bool check,
         PendingStep& pending, std::string& why);
     bool judge(PendingStep& pending, std::string& why);
@@ -171,6 +173,7 @@ private:
     cudaStream_t stream_ = nullptr;
     CUmodule module_ = nullptr;
     std::map<std::string, CUfunction> functions_;
+    std::map<std::string, int> resident_;
     CUdeviceptr params_ = 0;
     CUdeviceptr uniforms_ = 0;
     void* arena_ = nullptr;
