@@ -765,40 +765,47 @@ __device__ __forceinline__ float fe_limit_face(float r, float fi, float fj, doub
         // tiles before 8, under budgets that leave room for 3, then 2, then 1 CTA an SM. A pass that reads no other
         // plane (RZ = 0) starts at 2 stages: the explicit Heston gather (7 sources, 512 x 256) takes 0.39 ms a substep
         // on 128 planes with 2 stages against 0.65 with 4, which leave room for one CTA an SM only. With the plane carry
-        // the ring holds planes z and z + 1 and the one being fetched: the 512^3 heat gather (32-row tiles, 76 registers:
-        // 3 CTAs an SM) 4.84 TB/s with 3 stages, 4.77 with 4; forced to 64 registers for 4 CTAs an SM it spills, 4.37.
-        const int shallowest = rz == 0 ? 2 : (pb.zcarry ? rz + 2 : std::max(4, 2 * rz + 2));
-        // First, 32-row tiles when they leave room for 3 CTAs an SM (a warp then computes 4 rows of a plane, so the
-        // per-plane waits, barrier and ring bookkeeping are shared by 16 cells a lane): the 512^3 heat gather, 16-row
-        // tiles 4.15 TB/s (5 CTAs an SM), 24 rows 4.10, 32 rows 4.41 (3 CTAs), 32 rows with 5 stages 4.02, 40 rows 3.34.
-        {
-            std::size_t floats = 0;
-            for (const Source& s : pb.sources) floats += static_cast<std::size_t>(((128 + 2 * s.ax) * (32 + 2 * s.ry) + 31) / 32 * 32) * shallowest;
-            if (floats * 4 <= 75u * 1024 && 32 + 2 * rz < 256) {
-                L.ty = 32;
-                L.nst = shallowest;
-                L.smem = static_cast<unsigned>(floats * 4);
-                return true;
+        // the ring holds planes z and z + 1, and its 4 stages keep two planes in flight: the 512^3 heat gather (32-row
+        // tiles, 80 registers: 3 CTAs an SM whatever the ring) 5.24 TB/s with 4 stages, 5.08 with 3; the 43-term law at
+        // 512^3 16.8 ms a step against 17.1. Forced to 64 registers for a fourth CTA an SM (3 stages) it spills: slower.
+        // A carried pass that fits no budget with 4 stages tries 3.
+        auto fit = [&](int shallowest) {
+            // First, 32-row tiles when they leave room for 3 CTAs an SM (a warp then computes 4 rows of a plane, so the
+            // per-plane waits, barrier and ring bookkeeping are shared by 16 cells a lane): the 512^3 heat gather,
+            // 16-row tiles 4.15 TB/s (5 CTAs an SM), 24 rows 4.10, 32 rows 4.41 (3 CTAs), 32 rows with 5 stages 4.02,
+            // 40 rows 3.34 (before the plane carry).
+            {
+                std::size_t floats = 0;
+                for (const Source& s : pb.sources) floats += static_cast<std::size_t>(((128 + 2 * s.ax) * (32 + 2 * s.ry) + 31) / 32 * 32) * shallowest;
+                if (floats * 4 <= 75u * 1024 && 32 + 2 * rz < 256) {
+                    L.ty = 32;
+                    L.nst = shallowest;
+                    L.smem = static_cast<unsigned>(floats * 4);
+                    return true;
+                }
             }
-        }
-        for (const std::size_t budget : {72u * 1024, 110u * 1024, 200u * 1024}) {
-            for (const int ty : {16, 8}) {
-                for (int nst = shallowest; nst <= shallowest + 2; ++nst) {
-                    std::size_t floats = 0;
-                    for (const Source& s : pb.sources) {
-                        const int plane = ((128 + 2 * s.ax) * (ty + 2 * s.ry) + 31) / 32 * 32;
-                        floats += static_cast<std::size_t>(plane) * nst;
-                    }
-                    if (floats * 4 <= budget && ty + 2 * rz < 256) {
-                        L.ty = ty;
-                        L.nst = nst;
-                        L.smem = static_cast<unsigned>(floats * 4);
-                        return true;
+            for (const std::size_t budget : {72u * 1024, 110u * 1024, 200u * 1024}) {
+                for (const int ty : {16, 8}) {
+                    for (int nst = shallowest; nst <= shallowest + 2; ++nst) {
+                        std::size_t floats = 0;
+                        for (const Source& s : pb.sources) {
+                            const int plane = ((128 + 2 * s.ax) * (ty + 2 * s.ry) + 31) / 32 * 32;
+                            floats += static_cast<std::size_t>(plane) * nst;
+                        }
+                        if (floats * 4 <= budget && ty + 2 * rz < 256) {
+                            L.ty = ty;
+                            L.nst = nst;
+                            L.smem = static_cast<unsigned>(floats * 4);
+                            return true;
+                        }
                     }
                 }
             }
-        }
-        return false;
+            return false;
+        };
+        if (rz == 0) return fit(2);
+        if (pb.zcarry) return fit(rz + 3) || fit(rz + 2);
+        return fit(std::max(4, 2 * rz + 2));
     }
 
     // How far along x a value reads, everything it inlines included (a stage read by it is one load: 0).
