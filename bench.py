@@ -43,6 +43,12 @@ def measured_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def heat_workload(n):
+    """The headline workload's name, the same on both arms."""
+    return (f"heat law d T = diffuse(1, T), conserves T, {n}^3 fp32 a GPU (on N GPUs one {n} x {n} x {n}N lattice in "
+            f"z-slabs, halo planes over NCCL), h = 1/{n}, dt = 0.4 h^2/6 (1 substep), contracts checked every step")
+
+
 def profile_traffic(name):
     """dram bytes per launch of the dominant kernel from the committed ncu summary (profiles/<name>.md), or None."""
     path = os.path.join(ROOT, "profiles", name)
@@ -193,8 +199,7 @@ def run_reference_arm(args, world, rank):
         "impl": "reference", "metric": "7-pt stencil effective HBM GB/s (8 B/cell/step)", "value": gbs, "unit": "GB/s",
         "n_gpus": world, "steps": sample_steps, "warmup": 1, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"heat 7-pt diffuse(D=1,T) {n}^3 fp32, conserves T, 1 substep, contracts on",
-                   "cells": cells},
+        "config": {"workload": heat_workload(n), "cells_per_gpu": cells},
         "cpu_baseline": {"value": gbs, "unit": "GB/s", "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": gbs, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -1124,9 +1129,7 @@ def run_ours(args, world, rank, local):
         "value": value, "unit": "GB/s", "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic: sum of 4 seeded Gaussian blobs (numpy default_rng(rank))",
-        "config": {"workload": f"heat law d T = diffuse(1, T), conserves T, {n}^3 fp32 a GPU (on N GPUs one {n} x {n} x {n}N "
-                               f"lattice in z-slabs, halo planes over NCCL), h = 1/{n}, dt = 0.4 h^2/6 (1 substep), "
-                               f"contracts checked every step", "cells_per_gpu": cells,
+        "config": {"workload": heat_workload(n), "cells_per_gpu": cells,
                    "path": "fe_law_step (law text -> IR -> generated sm_100a TMA pass)",
                    "l2": "inputs larger than L2 (512 MiB a buffer)",
                    "handwritten_kernel_gbs": BYTES_PER_CELL * cells / (hand_ms * 1e-3) / 1e9},
