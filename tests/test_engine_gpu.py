@@ -65,16 +65,25 @@ def test_two_runs_are_bit_identical(cuda, path):
 
 def test_engine_heat_bit_identical_to_handwritten_kernel(cuda):
     """The generated step of `d T = diffuse(D, T)` and the hand-written kernel do the same arithmetic in the same order:
-    equal to the bit (the reference's own check: bench/stencil_bench.cpp:291-294)."""
+    equal to the bit (the reference's own check: bench/stencil_bench.cpp:291-294). 64^3 and 96^3 take the plain pass,
+    the rest the TMA slab pass with the plane carry: one plane a chunk up to 160^3, then chunks of several planes whose
+    later planes read plane z - 1 from the registers (256^3: 4 planes; 203 x 256 x 384: 5, the last chunk 3; 256 x 512
+    x 512: the length the fullest-last-wave rule picks)."""
     import torch
     from fieldcuda import kernels
     from fieldcuda.solver import Solver
     from oracle import heat as oh
-    for n in (64, 96, 128, 160):   # the first two take the plain pass, the last two the TMA slab pass
-        h = 1.0 / n
+    shapes = [(64, 64, 64), (96, 96, 96), (128, 128, 128), (160, 160, 160), (256, 256, 256), (203, 256, 384),
+              (256, 512, 512)]
+    for shape in shapes:
+        nz, ny, nx = shape
+        h = 1.0 / nx
         dt = 0.4 * h * h / 6.0
-        T0 = oh.gaussian_blobs(n, h, seed=3)
-        s = Solver(open(os.path.join(ROOT, "tests", "laws", "heat.law")).read(), n, n, n, h)
+        if nz == ny == nx:
+            T0 = oh.gaussian_blobs(nx, h, seed=3)
+        else:
+            T0 = np.random.default_rng(nz).uniform(0.0, 1.0, shape).astype(np.float32)
+        s = Solver(open(os.path.join(ROOT, "tests", "laws", "heat.law")).read(), nx, ny, nz, h)
         s.set_field("T", T0)
         a = torch.from_numpy(T0).cuda()
         b = torch.empty_like(a)
@@ -85,8 +94,10 @@ def test_engine_heat_bit_identical_to_handwritten_kernel(cuda):
             a, b = b, a
         torch.cuda.synchronize()
         got = s.values("T")
-        assert np.array_equal(got.view(np.uint32), a.cpu().numpy().view(np.uint32))
+        assert np.array_equal(got.view(np.uint32), a.cpu().numpy().view(np.uint32)), shape
         s.close()
+        del a, b, ws
+        torch.cuda.empty_cache()
 
 
 def test_conservation_violation_is_reported(cuda):
