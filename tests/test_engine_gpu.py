@@ -274,3 +274,31 @@ def test_wider_staging_changes_no_bit(cuda):
         s.close()
     for a, b in zip(out[0], out[1]):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_two_source_plane_carry_matches_the_oracle(cuda):
+    """`d T = diffuse(k, T)` with k a field: both sources are read one plane down at the cell's own column, so both ride
+    the plane carry; on 128 x 256 x 256 the pass's z-chunks hold several planes. Against the oracle (the reference's CPU
+    arithmetic restated) within the reference's per-op gate (2e-5, src/tests/cuda_parity_smoke.cpp:114-117)."""
+    from fieldcuda import solver as sv
+    from fieldcuda.solver import Solver
+    from oracle import law_cpu
+    law = ("field T init 0 range -1e9 1e9\nfield k init 1 range 0 10 static\nterm t\n  d T = diffuse(k, T)\n"
+           "  conserves T\n")
+    src = sv.cuda_source(law, 128, 256, 256, 1.0 / 128)
+    assert "NCARRY = 2;" in src
+    shape = (256, 256, 128)
+    rng = np.random.default_rng(21)
+    init = {"T": rng.uniform(-1, 1, shape).astype(np.float32), "k": rng.uniform(0.5, 2.0, shape).astype(np.float32)}
+    h, dt = 1.0 / 128, 0.05 / 128 ** 2
+    s = Solver(law, 128, 256, 256, h)
+    o = law_cpu.Solver(law_cpu.Law(json.loads(sv.ir_json(law))), shape, h)
+    for name, v in init.items():
+        s.set_field(name, v)
+        o.fields[name] = v.copy()
+    for _ in range(2):
+        s.step(dt)
+        o.step(dt)
+    got, want = s.values("T").astype(np.float64), o.fields["T"].astype(np.float64)
+    s.close()
+    assert float(np.abs(got - want).max()) <= 2e-5 * float(np.abs(want).max())
